@@ -1,0 +1,207 @@
+"""Seeded synthetic meshes and orientation grids for the orientation search.
+
+The workloads the orientation search is measured on are described by shape
+only (no mesh files ship with them), so they are generated here with numpy:
+
+* ``perturbed_icosphere`` -- a closed icosphere whose vertices are displaced
+  radially by a sum of seeded real spherical harmonics, optionally plus
+  Gaussian bumps and dents (the small "plain method" mesh: subdivision 4,
+  5,120 triangles, r = 50 mm, 6 harmonics of degree <= 3, amplitude 0.15;
+  the 82k-triangle solid: subdivision 6, 81,920 triangles, r = 80 mm,
+  harmonics of degree <= 8 at amplitude 0.25 and 4 bumps/dents with
+  sigma 10 mm and height +-20 mm).
+* ``ypr_grid`` -- the (yaw, pitch, roll) array in the layout the reference
+  Python surface builds with ``np.meshgrid(yaw, pitch, [0])`` + ravel
+  (cfms_tomo/tomo_dll_interface.py:38-43): pitch-major, yaw fastest,
+  float32 radians.
+
+A mesh is returned as :class:`MeshArrays`, the same float32/int32 arrays the
+reference hands to its C-ABI (tomo_dll_interface.py:59-70): vertices, vertex
+normals, faces, face normals, surface area and convex hull.  Vertex normals
+are area-weighted face-normal sums; they are inputs to the search, so the
+GPU path and the oracle always receive identical bytes.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+__all__ = ["MeshArrays", "icosphere", "perturbed_icosphere", "ypr_grid", "small_solid",
+           "solid_82k", "random_mesh", "mesh_from_arrays"]
+
+
+@dataclass
+class MeshArrays:
+    """Mesh arrays in the dtypes of the reference C-ABI."""
+
+    vertices: np.ndarray          # [V, 3] float32
+    faces: np.ndarray             # [T, 3] int32
+    vertex_normals: np.ndarray    # [V, 3] float32
+    face_normals: np.ndarray      # [T, 3] float32
+    area: float                   # total surface area (float64, cast to float32 at the ABI)
+    hull_vertices: np.ndarray = field(default_factory=lambda: np.zeros((0, 3), np.float32))
+    hull_faces: np.ndarray = field(default_factory=lambda: np.zeros((0, 3), np.int32))
+    hull_face_normals: np.ndarray = field(default_factory=lambda: np.zeros((0, 3), np.float32))
+    is_watertight: bool = True
+    name: str = "mesh"
+
+    @property
+    def n_tri(self) -> int:
+        return int(self.faces.shape[0])
+
+    @property
+    def n_vtx(self) -> int:
+        return int(self.vertices.shape[0])
+
+
+def _normals(v: np.ndarray, f: np.ndarray) -> tuple[np.ndarray, np.ndarray, float]:
+    v64 = v.astype(np.float64)
+    a, b, c = v64[f[:, 0]], v64[f[:, 1]], v64[f[:, 2]]
+    cr = np.cross(b - a, c - a)
+    dbl_area = np.linalg.norm(cr, axis=1)
+    fn = cr / np.maximum(dbl_area, 1e-300)[:, None]
+    vn = np.zeros_like(v64)
+    for k in range(3):
+        np.add.at(vn, f[:, k], cr)          # area-weighted
+    vn /= np.maximum(np.linalg.norm(vn, axis=1), 1e-300)[:, None]
+    return vn.astype(np.float32), fn.astype(np.float32), float(dbl_area.sum() * 0.5)
+
+
+def _hull(v: np.ndarray) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+    try:
+        from scipy.spatial import ConvexHull
+    except Exception:  # pragma: no cover - scipy is in the image
+        return (np.zeros((0, 3), np.float32), np.zeros((0, 3), np.int32), np.zeros((0, 3), np.float32))
+    h = ConvexHull(v.astype(np.float64))
+    used = np.unique(h.simplices)
+    remap = -np.ones(v.shape[0], np.int64)
+    remap[used] = np.arange(used.size)
+    hv = v[used].astype(np.float32)
+    hf = remap[h.simplices].astype(np.int32)
+    hn = h.equations[:, :3].astype(np.float32)
+    return hv, hf, hn
+
+
+def mesh_from_arrays(vertices, faces, name: str = "mesh", with_hull: bool = True,
+                     vertex_normals=None, watertight: bool | None = None) -> MeshArrays:
+    """Build :class:`MeshArrays` from raw vertices/faces."""
+    v = np.ascontiguousarray(vertices, dtype=np.float32)
+    f = np.ascontiguousarray(faces, dtype=np.int32)
+    vn, fn, area = _normals(v, f)
+    if vertex_normals is not None:
+        vn = np.ascontiguousarray(vertex_normals, dtype=np.float32)
+    hv, hf, hn = _hull(v) if (with_hull and v.shape[0] >= 4) else (
+        np.zeros((0, 3), np.float32), np.zeros((0, 3), np.int32), np.zeros((0, 3), np.float32))
+    if watertight is None:
+        watertight = _is_watertight(f)
+    return MeshArrays(v, f, vn, fn, area, hv, hf, hn, watertight, name)
+
+
+def _is_watertight(f: np.ndarray) -> bool:
+    e = np.sort(np.concatenate([f[:, [0, 1]], f[:, [1, 2]], f[:, [2, 0]]]), axis=1)
+    _, counts = np.unique(e, axis=0, return_counts=True)
+    return bool(np.all(counts == 2))
+
+
+def icosphere(subdivisions: int) -> tuple[np.ndarray, np.ndarray]:
+    """Unit icosphere: 20 * 4**subdivisions faces (float64 vertices)."""
+    t = (1.0 + 5 ** 0.5) / 2.0
+    v = [(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t), (0, -1, -t), (0, 1, -t),
+         (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)]
+    f = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2),
+         (10, 7, 6), (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5),
+         (2, 4, 11), (6, 2, 10), (8, 6, 7), (9, 8, 1)]
+    verts = np.array(v, np.float64)
+    verts /= np.linalg.norm(verts, axis=1)[:, None]
+    faces = np.array(f, np.int64)
+    for _ in range(subdivisions):
+        e = np.concatenate([faces[:, [0, 1]], faces[:, [1, 2]], faces[:, [2, 0]]])
+        es = np.sort(e, axis=1)
+        uniq, inv = np.unique(es, axis=0, return_inverse=True)
+        mids = verts[uniq[:, 0]] + verts[uniq[:, 1]]
+        mids /= np.linalg.norm(mids, axis=1)[:, None]
+        base = verts.shape[0]
+        verts = np.vstack([verts, mids])
+        inv = inv.reshape(3, -1).T + base          # [T, 3]: mid of (0,1), (1,2), (2,0)
+        a, b, c = faces[:, 0], faces[:, 1], faces[:, 2]
+        ab, bc, ca = inv[:, 0], inv[:, 1], inv[:, 2]
+        faces = np.concatenate([np.stack([a, ab, ca], 1), np.stack([b, bc, ab], 1),
+                                np.stack([c, ca, bc], 1), np.stack([ab, bc, ca], 1)])
+    return verts, faces
+
+
+def _real_sh(l: int, m: int, theta: np.ndarray, phi: np.ndarray) -> np.ndarray:
+    from scipy.special import sph_harm_y
+    if m == 0:
+        return np.real(sph_harm_y(l, 0, theta, phi))
+    y = sph_harm_y(l, abs(m), theta, phi)
+    s = np.sqrt(2.0) * (-1.0) ** m
+    return s * (np.real(y) if m > 0 else np.imag(y))
+
+
+def perturbed_icosphere(subdivisions: int, radius: float, seed: int, n_harmonics: int = 6,
+                        max_degree: int = 3, amplitude: float = 0.15, n_bumps: int = 0,
+                        bump_sigma: float = 10.0, bump_height: float = 20.0, scale: float = 1.0,
+                        name: str | None = None, with_hull: bool = True) -> MeshArrays:
+    """Closed icosphere, radially displaced by seeded real spherical harmonics
+    (and optionally Gaussian bumps/dents), coordinates multiplied by ``scale``
+    (2.0 expresses 0.5 mm voxels on the reference's 1-unit grid)."""
+    rng = np.random.default_rng(seed)
+    u, f = icosphere(subdivisions)
+    theta = np.arccos(np.clip(u[:, 2], -1.0, 1.0))
+    phi = np.arctan2(u[:, 1], u[:, 0])
+    s = np.zeros(u.shape[0])
+    for _ in range(n_harmonics):
+        l = int(rng.integers(1, max_degree + 1))
+        m = int(rng.integers(-l, l + 1))
+        s += rng.uniform(-1.0, 1.0) * _real_sh(l, m, theta, phi)
+    r = radius * (1.0 + amplitude * s)
+    for _ in range(n_bumps):
+        c = rng.normal(size=3)
+        c /= np.linalg.norm(c)
+        h = bump_height * (1.0 if rng.random() < 0.5 else -1.0)
+        d2 = np.sum((u * radius - c * radius) ** 2, axis=1)
+        r = r + h * np.exp(-d2 / (2.0 * bump_sigma ** 2))
+    r = np.maximum(r, 0.05 * radius)
+    v = (u * r[:, None]) * scale
+    return mesh_from_arrays(v, f, name or f"ico{subdivisions}_s{seed}", with_hull=with_hull, watertight=True)
+
+
+def small_solid(seed: int = 0, with_hull: bool = True) -> MeshArrays:
+    """Plain-method mesh: subdivision 4 (5,120 triangles), r = 50 mm, 1 mm voxels."""
+    return perturbed_icosphere(4, 50.0, seed, n_harmonics=6, max_degree=3, amplitude=0.15,
+                               name=f"solid5k_s{seed}", with_hull=with_hull)
+
+
+def solid_82k(seed: int = 0, with_hull: bool = True) -> MeshArrays:
+    """82k-triangle solid: subdivision 6 (81,920 triangles), r = 80 mm, SH degree <= 8 at
+    amplitude 0.25 plus 4 Gaussian bumps/dents (sigma 10 mm, +-20 mm), 0.5 mm voxels
+    (coordinates x2)."""
+    return perturbed_icosphere(6, 80.0, seed, n_harmonics=12, max_degree=8, amplitude=0.25,
+                               n_bumps=4, bump_sigma=10.0, bump_height=20.0, scale=2.0,
+                               name=f"solid82k_s{seed}", with_hull=with_hull)
+
+
+def random_mesh(n_tri: int, seed: int, extent: float = 60.0, open_fraction: float = 0.0) -> MeshArrays:
+    """Triangle soup for edge-case tests: random small and sliver triangles
+    (not watertight)."""
+    rng = np.random.default_rng(seed)
+    centers = rng.uniform(0.2 * extent, 0.8 * extent, size=(n_tri, 3))
+    sizes = rng.lognormal(mean=0.0, sigma=1.0, size=(n_tri, 1))
+    offs = rng.normal(size=(n_tri, 3, 3)) * sizes[:, :, None]
+    sliver = rng.random(n_tri) < 0.15
+    offs[sliver, 2, :] = offs[sliver, 1, :] * rng.uniform(-1.2, 1.2, size=(int(sliver.sum()), 1))
+    v = (centers[:, None, :] + offs).reshape(-1, 3)
+    f = np.arange(3 * n_tri, dtype=np.int32).reshape(-1, 3)
+    return mesh_from_arrays(v, f, f"soup{n_tri}_s{seed}", with_hull=True, watertight=False)
+
+
+def ypr_grid(yaw_deg, pitch_deg, roll_deg=(0.0,)) -> np.ndarray:
+    """[n, 3] float32 radians, pitch-major / yaw-fastest like the reference's
+    np.meshgrid(yaw, pitch, roll) + ravel (tomo_dll_interface.py:38-43)."""
+    yaw = np.asarray(yaw_deg, np.float64) * np.pi / 180.0
+    pitch = np.asarray(pitch_deg, np.float64) * np.pi / 180.0
+    roll = np.asarray(roll_deg, np.float64) * np.pi / 180.0
+    xx, yy, zz = np.meshgrid(yaw.astype(np.float32), pitch.astype(np.float32), roll.astype(np.float32))
+    return np.ascontiguousarray(np.column_stack([xx.ravel(), yy.ravel(), zz.ravel()]).astype(np.float32))
