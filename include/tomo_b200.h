@@ -1,0 +1,120 @@
+/*
+ * tomo_b200.h -- C-ABI of libtomo_b200.so, the B200 (sm_100a) orientation
+ * search of cfms-lab/Tomo_Shell2026.
+ *
+ * The first block is a drop-in for the reference DLL exports
+ * (cfms_tomo/Tomo_Shell_vc_src/Tomo_Shell2026.h:19-35) as bound by the
+ * reference Python surface through ctypes (cfms_tomo/tomo_dll_interface.py:23-43,
+ * cfms_tomo/shell_test/tomoSh_Cpp.py:67-120).  Same names, argument order and
+ * meaning; MESH_ELE_ID_TYPE is int32, FLOAT32 is float, INT16 is short.
+ * Differences: errors return negative codes instead of terminating the
+ * process, results are exact (int64 totals are exported next to the float
+ * ones), and the library never calls cudaDeviceReset.
+ *
+ * All buffers returned by getters are owned by the library and stay valid
+ * until the next TomoSh_CUDA call or OnDestroy.  Calls are serialised by an
+ * internal lock; one process drives one GPU (the current CUDA device).
+ */
+#ifndef TOMO_B200_H
+#define TOMO_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* error codes (returned by TomoSh_CUDA and the tomo* calls; 0 or an index on success) */
+#define TOMO_ERR_ARG (-1)       /* bad argument (null pointer, negative size, index out of range) */
+#define TOMO_ERR_CUDA (-2)      /* CUDA runtime error, see tomoGetLastErrorString */
+#define TOMO_ERR_CAPACITY (-3)  /* a fixed capacity was exceeded (grid, shared-memory column strip) */
+
+/* ---- reference-compatible exports ---------------------------------------- */
+
+/* Exhaustive orientation search.  Replaces TomoSh_CUDA / TomoSh_INT3
+ * (Tomo_Shell2026.h:33-35, Tomo_Shell2026.cpp:296-299,367-417).
+ *   f32info[12]  dVoxel, theta_c, surface_area, wall_thickness, Fcore, Fclad,
+ *                Fss, Css, PLA_density, BedInnerBound, BedOuterBound, BedThickness
+ *                (S3DPrinterInfo.h:42-47)
+ *   i32info[11]  bVerbose, bUseExplicitSS, bShellMesh, nVoxel, nTri, nVtx, nYPR,
+ *                nHullTri, nHullVtx, BedType, ShellThickness*1000 (S3DPrinterInfo.cpp:132-144)
+ *   YPR[nYPR*3]  yaw, pitch, roll in radians
+ *   tri[nTri*3], vtx[nVtx*3], vtx_nrm[nVtx*3]  mesh; tri_nrm and the convex
+ *                hull arrays are accepted and unused (the INT3 arithmetic does
+ *                not read them).
+ * Returns optID = first index of the strictly smallest Mss starting from
+ * 1e5 (_find1stOptimal, Tomo_Shell2026.cpp:128-136), or a negative error. */
+int TomoSh_CUDA(float* f32info, int* i32info, float* YPR, int* tri, float* vtx, float* vtx_nrm, float* tri_nrm,
+                int* chull_tri, float* chull_vtx, float* chull_trinrm);
+
+/* getMss / getMo / getVtc: [nYPR] float32 (Tomo_Shell2026.h:21-23). */
+float* getMss(void);
+float* getMo(void);
+float* getVtc(void);
+/* 22-float vm_info of the best orientation (Tomo_Shell2026.h:24, STomoVolMassInfo.h:19-33). */
+float* getVolMassInfo(void);
+/* 4x4 transform of the best orientation (Tomo_Shell2026.h:25, STomoSh_Base.cpp:155-167). */
+float* getMat4x4(void);
+/* Render pixels of the best orientation by enumPixelType (Tomo_Shell2026.h:19-20);
+ * n x 6 int16 (x, y, z, nx, ny, nz). */
+int getnData2i(short type);
+short* getpData2i(short type);
+/* Frees every library buffer and the device work memory (Tomo_Shell2026.h:29). */
+void OnDestroy(void);
+
+/* ---- additions -------------------------------------------------------------- */
+
+/* Exact per-orientation totals [nYPR] of the last call: sum of per-column
+ * Vo / Vss / Vtc in int64 (the reference keeps them in float32,
+ * STomoVolMassInfo.h:24-31; its own debug accumulator is int64,
+ * STomoSh_INT3.cpp:129-170). */
+const long long* getVo64(void);
+const long long* getVss64(void);
+const long long* getVtc64(void);
+
+int tomoGetLastError(void);
+const char* tomoGetLastErrorString(void);
+
+/* Host-side pieces, exported so tests can pin them to the reference:
+ * rotation of SMatrix4f::YPR (SMatrix4f.cpp:213-240), 3x3 row-major;
+ * shadow threshold of STomoSh_INT3.cpp:756; VolToMass of STomoVolMassInfo.cpp:42-80. */
+void tomoRotation(float yaw, float pitch, float roll, float* out9);
+float tomoShadowThreshold(float theta_c);
+void tomoVolToMass(const float* f32info, const int* i32info, float* vm22);
+
+/* Tuning / test hooks. */
+#define TOMO_OPT_BATCH 1        /* orientations per device batch (default 64) */
+#define TOMO_OPT_STRIP_H 2      /* force strip height 1, 2, 4 or 8 (0 = automatic) */
+#define TOMO_OPT_FORCE_SAFE 3   /* 1 = evaluate every orientation in safe mode */
+int tomoSetOption(int key, int value);
+
+/* out[0..7] = grid edge, strip height, strips, entry capacity, safe re-runs, nYPR, batch, 0 */
+int tomoGetStats(long long* out, int n);
+
+/* Per-orientation results of the last sweep; any pointer may be null. */
+int tomoGetResults(long long* vo64, long long* vss64, long long* vtc64, float* vof, float* vssf, float* vtcf,
+                   int* nbed, int* flags, long long* entries, long long* columns);
+
+/* Split form of TomoSh_CUDA: upload the mesh and orientations once, run the
+ * device sweep any number of times with the inputs resident in device memory
+ * (optionally bracketed by caller-created cudaEvent_t handles; kernel_ms
+ * receives the elapsed device time), then finish on the host. */
+int tomoPrepare(const float* f32info, const int* i32info, const float* YPR, const int* tri, const float* vtx,
+                const float* vtx_nrm);
+int tomoSweepDevice(void* ev_start, void* ev_stop, float* kernel_ms);
+int tomoFinish(float* Mo, float* Mss, float* Vtc);
+
+/* Slot grid edge G of the prepared mesh (slot id = x * G + y). */
+int tomoGridSize(void);
+
+/* One orientation of the prepared sweep with a dense per-column dump (parity
+ * tests; no reference counterpart -- the reference writes comparable CSV
+ * dumps behind TOMO_DEBUG_PAIR_OUTPUT, STomoSh_INT3.cpp:172-235).
+ *   cols8[G*G*8]    n_distinct, n_final, vo, vss, tc, last_z, last_type, bed flags
+ *   keys64[G*G*64]  kept (z, nz) keys, (z+32768)<<16 | (nz+32768), in column order
+ *   types64[G*G*64] their type bits after pairing
+ * Returns the orientation's status flags (>= 0) or a negative error. */
+int tomoColumnDump(int ypr_index, int safe_mode, int* cols8, unsigned* keys64, short* types64);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,174 @@
+"""CUDA path vs the oracle, through the C-ABI (TomoSh_CUDA and the split
+entry points).  Integer outputs and the reference's float32 outputs are
+compared bit for bit."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from tomo_shell2026_b200 import meshgen, native
+from tomo_shell2026_b200.options import PrintOptions
+
+pytestmark = pytest.mark.gpu
+
+FLOAT_KEYS = ("Mo", "Mss", "Vtc")
+
+
+def _same_bits(a, b):
+    a = np.asarray(a); b = np.asarray(b)
+    if a.dtype == np.float32:
+        return np.array_equal(a.view(np.int32), b.view(np.int32))
+    return np.array_equal(a, b)
+
+
+def _compare(res, ora, label=""):
+    assert _same_bits(res.Vo64, ora["Vo64"]), f"{label} Vo64 differs at {np.nonzero(res.Vo64 != ora['Vo64'])[0][:10]}"
+    assert _same_bits(res.Vss64, ora["Vss64"]), f"{label} Vss64 differs at {np.nonzero(res.Vss64 != ora['Vss64'])[0][:10]}"
+    assert _same_bits(res.Vtc64, ora["Vtc64"]), f"{label} Vtc64 differs"
+    assert _same_bits(res.VoF, ora["VoF"]), f"{label} VoF differs"
+    assert _same_bits(res.VssF, ora["VssF"]), f"{label} VssF differs"
+    for k in FLOAT_KEYS:
+        assert _same_bits(getattr(res, k), ora[k]), f"{label} {k} differs at {np.nonzero(getattr(res, k) != ora[k])[0][:10]}"
+    assert res.optID == ora["optID"], f"{label} optID {res.optID} != {ora['optID']}"
+    assert np.array_equal(res.entries, ora["entries"]), f"{label} entry counts differ"
+    assert np.array_equal(res.columns, ora["columns"]), f"{label} occupied-column counts differ"
+
+
+GRID_SMALL = meshgen.ypr_grid(np.arange(0, 360, 30), np.arange(0, 190, 30))
+
+
+@pytest.mark.parametrize("explicit_ss", [True, False])
+def test_small_solid_sweep(oracle, explicit_ss):
+    m = meshgen.small_solid(0)
+    ypr = meshgen.ypr_grid(np.arange(0, 360, 10), np.arange(0, 190, 10))
+    opts = PrintOptions(explicit_ss=explicit_ss)
+    _compare(native.sweep(m, ypr, opts), oracle.sweep(m, ypr, opts), "small solid")
+
+
+@pytest.mark.parametrize("bed", [(1, 0.0, 2.0, 0.97), (2, 0.0, 2.0, 0.97), (3, 1.0, 3.0, 0.97), (2, 0.0, 5.5, 1.3)])
+@pytest.mark.parametrize("explicit_ss", [True, False])
+def test_bed_types(oracle, bed, explicit_ss):
+    m = meshgen.small_solid(1)
+    bt, bi, bo, th = bed
+    opts = PrintOptions(explicit_ss=explicit_ss, bed_type=bt, bed_inner=bi, bed_outer=bo, bed_thickness=th)
+    _compare(native.sweep(m, GRID_SMALL, opts), oracle.sweep(m, GRID_SMALL, opts), f"bed {bed}")
+
+
+@pytest.mark.parametrize("thickness", [0.5, 2.3])
+def test_shell_mode(oracle, thickness):
+    m = meshgen.small_solid(2)
+    opts = PrintOptions(explicit_ss=True, shell_mesh=True, shell_thickness=thickness, bed_type=2, bed_outer=2.0,
+                        bed_thickness=0.97)
+    _compare(native.sweep(m, GRID_SMALL, opts), oracle.sweep(m, GRID_SMALL, opts), "shell")
+
+
+@pytest.mark.parametrize("explicit_ss", [True, False])
+def test_triangle_soup_slivers(oracle, explicit_ss):
+    s = meshgen.random_mesh(3000, 5)
+    opts = PrintOptions(explicit_ss=explicit_ss, shell_mesh=True, bed_type=2, bed_outer=2.0, bed_thickness=0.97)
+    _compare(native.sweep(s, GRID_SMALL, opts), oracle.sweep(s, GRID_SMALL, opts), "soup")
+
+
+def _layers(n_layers=45, n=12, seed=3):
+    rng = np.random.default_rng(seed)
+    V, F = [], []
+    for L in range(n_layers):
+        xs, ys = np.meshgrid(np.linspace(20, 80, n), np.linspace(20, 80, n), indexing="ij")
+        zs = 10 + L * 2.3 + 0.8 * np.sin(xs * 0.3 + L) + 0.5 * rng.standard_normal(xs.shape)
+        base = len(V)
+        V += list(np.stack([xs.ravel(), ys.ravel(), zs.ravel()], 1))
+        for i in range(n - 1):
+            for j in range(n - 1):
+                a = base + i * n + j
+                b, c, d = a + 1, a + n, a + n + 1
+                F += [(a, c, b), (b, c, d)] if L % 2 else [(a, b, c), (b, d, c)]
+    return meshgen.mesh_from_arrays(np.array(V), np.array(F), "layers")
+
+
+@pytest.mark.parametrize("shell", [False, True])
+def test_slot_cap_truncation(oracle, shell):
+    m = _layers()
+    ypr = meshgen.ypr_grid(np.arange(0, 360, 45), np.arange(0, 60, 20))
+    opts = PrintOptions(explicit_ss=True, shell_mesh=shell, bed_type=2, bed_outer=2.0, bed_thickness=0.97)
+    _compare(native.sweep(m, ypr, opts), oracle.sweep(m, ypr, opts), "layers")
+
+
+@pytest.mark.parametrize("h", [1, 2, 4, 8])
+def test_strip_heights_agree(oracle, h):
+    m = meshgen.small_solid(3)
+    opts = PrintOptions(explicit_ss=True, bed_type=2, bed_outer=2.0, bed_thickness=0.97)
+    native.set_option(native.TOMO_OPT_STRIP_H, h)
+    try:
+        res = native.sweep(m, GRID_SMALL, opts)
+    finally:
+        native.set_option(native.TOMO_OPT_STRIP_H, 0)
+    _compare(res, oracle.sweep(m, GRID_SMALL, opts), f"H={h}")
+
+
+def test_safe_mode_agrees(oracle):
+    m = meshgen.small_solid(4)
+    opts = PrintOptions(explicit_ss=False, shell_mesh=True, bed_type=1, bed_outer=2.0, bed_thickness=0.97)
+    native.set_option(native.TOMO_OPT_FORCE_SAFE, 1)
+    try:
+        res = native.sweep(m, GRID_SMALL, opts)
+    finally:
+        native.set_option(native.TOMO_OPT_FORCE_SAFE, 0)
+    _compare(res, oracle.sweep(m, GRID_SMALL, opts), "safe")
+
+
+def test_columns_match_oracle(oracle):
+    m = meshgen.small_solid(0)
+    ypr = GRID_SMALL
+    opts = PrintOptions(explicit_ss=True, shell_mesh=True, bed_type=2, bed_outer=2.0, bed_thickness=0.97)
+    sess = native.Session(m, ypr, opts)
+    G = sess.grid()
+    assert G == 256
+    for idx in (0, 7, 40):
+        for safe in (False, True):
+            d = sess.columns(idx, safe=safe)
+            o = oracle.columns(m, ypr, opts, idx, grid=G)
+            nd = d["cols"][:, 0]
+            # distinct pixel count after voxelization, per column
+            assert np.array_equal(nd, np.minimum(o["n_vox"], 63)), f"n_vox differs (idx {idx}, safe {safe})"
+            # pixel count after pairing (floor sentinels)
+            occ = nd > 0
+            bed_free = o["n_fin"].copy()
+            assert np.array_equal(d["cols"][occ, 2], o["col_vo"][occ]), "per-column Vo differs"
+            assert np.array_equal(d["cols"][occ, 3], o["col_vss"][occ]), "per-column Vss differs"
+            # kept keys in column order against the oracle's sorted rows
+            for s in np.nonzero(nd > 1)[0][:2000]:
+                n = nd[s]
+                z = (d["keys"][s, :n] >> 16).astype(np.int64) - 32768
+                nz = (d["keys"][s, :n] & 0xFFFF).astype(np.int64) - 32768
+                oz = o["fin_tzn"][s, :n, 1]
+                onz = o["fin_tzn"][s, :n, 2]
+                assert np.array_equal(z, oz) and np.array_equal(nz, onz), f"column {s} keys differ"
+                ot = o["fin_tzn"][s, :n, 0] & ~32  # bed bit is added after pairing
+                assert np.array_equal(d["types"][s, :n], ot), f"column {s} types differ"
+            del bed_free
+
+
+def test_repeat_runs_identical():
+    m = meshgen.small_solid(5)
+    opts = PrintOptions(explicit_ss=True, shell_mesh=True)
+    a = native.sweep(m, GRID_SMALL, opts)
+    b = native.sweep(m, GRID_SMALL, opts)
+    assert _same_bits(a.Mss, b.Mss) and np.array_equal(a.Vss64, b.Vss64) and a.optID == b.optID
+
+
+def test_large_grid_solid(oracle):
+    m = meshgen.solid_82k(0)
+    ypr = meshgen.ypr_grid(np.arange(0, 360, 90), np.arange(0, 61, 30))
+    opts = PrintOptions(explicit_ss=True)
+    res = native.sweep(m, ypr, opts)
+    st = native.stats()
+    assert st["grid"] > 256
+    _compare(res, oracle.sweep(m, ypr, opts, grid=st["grid"]), "82k")
+
+
+def test_bad_index_is_an_error():
+    m = meshgen.small_solid(0)
+    bad = meshgen.MeshArrays(m.vertices, m.faces.copy(), m.vertex_normals, m.face_normals, m.area)
+    bad.faces[5, 1] = m.n_vtx + 10
+    with pytest.raises(native.TomoError):
+        native.sweep(bad, GRID_SMALL, PrintOptions())

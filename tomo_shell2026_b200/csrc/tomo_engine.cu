@@ -1,0 +1,841 @@
+// Host side of the B200 orientation-search engine and its C-ABI.
+//
+// The C-ABI mirrors the reference DLL exports (Tomo_Shell_vc_src/Tomo_Shell2026.h:19-35):
+// TomoSh_CUDA takes the same ten pointers and returns optID; the getters return
+// library-owned buffers valid until the next call or OnDestroy.  Errors are
+// returned as negative codes (tomoGetLastError / tomoGetLastErrorString)
+// instead of the reference's exit(0) on CUDA failure (cuda_src/CUDA_types.cuh:112-118).
+//
+// Work split: rotation matrices, the shadow threshold and the mass model are
+// evaluated on the host with the same C library calls as the reference
+// (SMatrix4f::YPR, STomoSh_INT3.cpp:756, STomoVolMassInfo::VolToMass), so those
+// floats are bit-identical by construction; everything per vertex, triangle,
+// pixel and column runs in the kernels of tomo_kernels.cu.
+#include "tomo_common.cuh"
+#include "../../include/tomo_b200.h"
+
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+namespace tomo {
+
+size_t strip_smem_bytes(int H, int G, int ent_cap);
+cudaError_t configure_kernels(size_t strip_smem);
+cudaError_t launch_batch(const EngineParams& p, cudaStream_t main, size_t strip_smem);
+cudaError_t launch_fold(const EngineParams& p, cudaStream_t side);
+cudaError_t launch_bin_count(const EngineParams& p, cudaStream_t main);
+cudaError_t launch_after_count(const EngineParams& p, cudaStream_t main, size_t strip_smem);
+
+namespace {
+
+std::mutex g_mutex;
+int g_last_error = 0;
+std::string g_last_error_str;
+
+int set_error(int code, const std::string& msg)
+{
+  g_last_error = code;
+  g_last_error_str = msg;
+  return code;
+}
+
+#define TOMO_CUDA(call)                                                                  \
+  do {                                                                                   \
+    cudaError_t e_ = (call);                                                             \
+    if (e_ != cudaSuccess)                                                               \
+      return set_error(TOMO_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+#define TOMO_TRY(call)        \
+  do {                        \
+    const int rc_ = (call);   \
+    if (rc_ != 0) return rc_; \
+  } while (0)
+
+// ------------------------------------------------ host arithmetic (bit-exact with the reference)
+
+// SMatrix4f::YPR (cpu_src/SMatrix4f.cpp:213-240), 3x3 block row-major.
+void rotation(float ga, float be, float al, float R[9])
+{
+  const float cos_al = cosf(al), cos_be = cosf(be), cos_ga = cosf(ga);
+  const float sin_al = sinf(al), sin_be = sinf(be), sin_ga = sinf(ga);
+  R[0] = cos_al * cos_be;
+  R[1] = cos_al * sin_be * sin_ga - sin_al * cos_ga;
+  R[2] = cos_al * sin_be * cos_ga + sin_al * sin_ga;
+  R[3] = sin_al * cos_be;
+  R[4] = sin_al * sin_be * sin_ga + cos_al * cos_ga;
+  R[5] = sin_al * sin_be * cos_ga - cos_al * sin_ga;
+  R[6] = -sin_be;
+  R[7] = cos_be * sin_ga;
+  R[8] = cos_be * cos_ga;
+}
+
+struct Params {
+  float dVoxel, theta_c, surface_area, wall, Fcore, Fclad, Fss, Css, rho;
+  float bed_inner, bed_outer, bed_thickness;
+  int explicit_ss, shell, n_tri, n_vtx, n_ypr, bed_type;
+  float shell_thickness;
+};
+
+// S3DPrinterInfo::Set (cpu_src/S3DPrinterInfo.cpp:130-144)
+Params read_params(const float* f, const int* i)
+{
+  Params p;
+  p.dVoxel = f[0]; p.theta_c = f[1]; p.surface_area = f[2]; p.wall = f[3];
+  p.Fcore = f[4]; p.Fclad = f[5]; p.Fss = f[6]; p.Css = f[7]; p.rho = f[8];
+  p.bed_inner = f[9]; p.bed_outer = f[10]; p.bed_thickness = f[11];
+  p.explicit_ss = ((float)i[1] > 0.001f);
+  p.shell = ((float)i[2] > 0.001f);
+  p.shell_thickness = (float)i[10] * 0.001f;
+  p.n_tri = i[4]; p.n_vtx = i[5]; p.n_ypr = i[6]; p.bed_type = i[9];
+  return p;
+}
+
+// STomoVolMassInfo::VolToMass (cpu_src/STomoVolMassInfo.cpp:42-80); vm in
+// the 22-float vm_info layout (STomoVolMassInfo.h:19-33).
+void vol_to_mass(const Params& P, float* vm)
+{
+  const float Vss = vm[4], Vo = vm[8], Vbed = vm[11];
+  const float Vo_clad = P.surface_area * P.wall;
+  const float Vo_core = Vo - Vo_clad;
+  const float Mo_clad = Vo_clad * P.Fclad * P.rho;
+  const float Mo_core = Vo_core * P.Fcore * P.rho;
+  const float Mo = Mo_core + Mo_clad;
+  float Vss_clad = 0.f, Vss_core = 0.f, Ass_clad = 0.f, Mss_clad = 0.f, Mss_core = 0.f, Mss = 0.f;
+  if (P.explicit_ss) {
+    if (Vss > 0.001f) {
+      const float radius = powf(Vss / (4.f / 3.f * 3.141592f), 1.f / 3.f);
+      Ass_clad = (float)(4. * 3.141592 * (double)radius * (double)radius);
+      Vss_clad = Ass_clad * P.wall;
+      if (Vss_clad > Vss) Vss_clad = Vss;
+      Vss_core = Vss - Vss_clad;
+      Mss_clad = Vss_clad * P.Fclad * P.rho;
+      Mss_core = Vss_core * P.Fcore * P.rho;
+      Mss = Mss_core + Mss_clad;
+    }
+  } else {
+    Mss = Vss * P.Fss * P.Css * P.rho;
+  }
+  const float Mbed = Vbed * P.wall * P.rho;
+  Mss += Mbed;
+  vm[5] = Vss_clad; vm[6] = Vss_core; vm[7] = Ass_clad;
+  vm[9] = Vo_clad; vm[10] = Vo_core;
+  vm[12] = Mbed;
+  vm[13] = Mss; vm[14] = Mss_clad; vm[15] = Mss_core;
+  vm[16] = Mo; vm[17] = Mo_clad; vm[18] = Mo_core;
+  vm[19] = Mo + Mss;
+}
+
+// _find1stOptimal (Tomo_Shell2026.cpp:128-136)
+int first_optimal(int n, const float* mss)
+{
+  if (n <= 1) return 0;
+  int idx = 0;
+  float best = 1e5f;
+  for (int i = 0; i < n; i++)
+    if (mss[i] < best) { best = mss[i]; idx = i; }
+  return idx;
+}
+
+float largest_float_not_above(double c)
+{
+  float f = (float)c;
+  while ((double)f > c) f = nextafterf(f, -INFINITY);
+  while ((double)nextafterf(f, INFINITY) <= c) f = nextafterf(f, INFINITY);
+  return f;
+}
+
+template <typename T>
+struct DevBuf {
+  T* ptr = nullptr;
+  size_t n = 0;
+  cudaError_t reserve(size_t count)
+  {
+    if (count <= n && ptr) return cudaSuccess;
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr; n = 0;
+    cudaError_t e = cudaMalloc((void**)&ptr, sizeof(T) * (count ? count : 1));
+    if (e == cudaSuccess) n = count;
+    return e;
+  }
+  void release() { if (ptr) cudaFree(ptr); ptr = nullptr; n = 0; }
+};
+
+// Largest slot grid edge (columns of the rotated footprint at the voxel pitch).
+constexpr int kMaxGrid = 4096;
+
+struct BatchSet {   // per-batch buffers read by the fold, double-buffered
+  DevBuf<long long> acc;
+  DevBuf<int> flags;
+  DevBuf<int> foldcnt;
+  DevBuf<int4> foldv;
+  cudaEvent_t folded = nullptr;
+};
+
+}  // namespace
+
+// ------------------------------------------------ engine
+
+struct Engine {
+  int device = -1;
+  cudaStream_t main = nullptr, side = nullptr;
+  cudaEvent_t ev_ready = nullptr;
+  size_t smem_optin = 0;
+
+  // mesh and orientations
+  DevBuf<float4> vpos, vnrm;
+  DevBuf<int4> tri;
+  DevBuf<float> rot;
+  DevBuf<int> ori;
+  // batch work buffers
+  DevBuf<float4> xf;
+  DevBuf<unsigned> minkey;
+  DevBuf<uint8_t> tcode;
+  DevBuf<int> bin_off, bin_cur, bins, bbox;
+  DevBuf<uint8_t> bedf;
+  BatchSet set[2];
+  // outputs
+  DevBuf<long long> o_vo, o_vss, o_vtc, o_ent, o_col;
+  DevBuf<float> o_vof, o_vssf, o_vtcf;
+  DevBuf<int> o_nbed, o_flags;
+  // dump
+  DevBuf<int> dump_cols;
+  DevBuf<unsigned> dump_keys;
+  DevBuf<short> dump_types;
+
+  // host results of the last sweep
+  Params P{};
+  int nYPR = 0, G = 0, H = 0, S = 0, ent_cap = 0;
+  int batch = 64;
+  int force_h = 0;        // test hook: strip height override
+  int force_safe = 0;     // test hook: run every orientation in safe mode
+  float cx = 0, cy = 0, cz = 0;
+  std::vector<float> h_rot;
+  std::vector<long long> vo64, vss64, vtc64, entries, columns;
+  std::vector<float> vof, vssf, vtcf, Mo, Mss, Vtc;
+  std::vector<int> nbed, flags;
+  float volmass[22] = {0};
+  float mat4x4[16] = {0};
+  double last_kernel_ms = 0.0;
+  int n_safe = 0;
+
+  int init()
+  {
+    if (main) return 0;
+    int dev = 0;
+    TOMO_CUDA(cudaGetDevice(&dev));
+    device = dev;
+    TOMO_CUDA(cudaStreamCreateWithFlags(&main, cudaStreamNonBlocking));
+    TOMO_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+    TOMO_CUDA(cudaEventCreateWithFlags(&ev_ready, cudaEventDisableTiming));
+    for (auto& s : set) TOMO_CUDA(cudaEventCreateWithFlags(&s.folded, cudaEventDisableTiming));
+    int optin = 0;
+    TOMO_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    smem_optin = (size_t)optin;
+    return 0;
+  }
+
+  void release()
+  {
+    vpos.release(); vnrm.release(); tri.release(); rot.release(); ori.release();
+    xf.release(); minkey.release(); tcode.release(); bin_off.release(); bin_cur.release(); bins.release();
+    bbox.release(); bedf.release();
+    for (auto& s : set) { s.acc.release(); s.flags.release(); s.foldcnt.release(); s.foldv.release(); }
+    o_vo.release(); o_vss.release(); o_vtc.release(); o_ent.release(); o_col.release();
+    o_vof.release(); o_vssf.release(); o_vtcf.release(); o_nbed.release(); o_flags.release();
+    dump_cols.release(); dump_keys.release(); dump_types.release();
+    if (main) { cudaStreamDestroy(main); main = nullptr; }
+    if (side) { cudaStreamDestroy(side); side = nullptr; }
+    if (ev_ready) { cudaEventDestroy(ev_ready); ev_ready = nullptr; }
+    for (auto& s : set) if (s.folded) { cudaEventDestroy(s.folded); s.folded = nullptr; }
+  }
+
+  // Grid edge: the reference grid is 256 x 256 (STomoVoxelSpaceInfo.h:10).
+  // Keep it whenever the rotated mesh fits, so every bounded result
+  // (including the bed window clipping at the grid edge) is the reference's;
+  // grow it otherwise (the reference would write out of bounds there).
+  int choose_grid(const float* vtx, int nV)
+  {
+    double r2 = 0.0;
+    for (int v = 0; v < nV; v++) {
+      const double dx = (double)vtx[v * 3 + 0] - cx, dy = (double)vtx[v * 3 + 1] - cy, dz = (double)vtx[v * 3 + 2] - cz;
+      r2 = std::max(r2, dx * dx + dy * dy + dz * dz);
+    }
+    const double span = 2.0 * std::sqrt(r2) * 1.004 + std::max(0.0, (double)P.bed_outer) + 6.0;
+    if (span <= 256.0) return 256;
+    return (int)span + (int)std::max(0.0f, P.bed_outer) + 2;
+  }
+
+  void choose_strips(int mode)
+  {
+    const size_t budget = std::min<size_t>(smem_optin ? smem_optin : 232448, 110 * 1024);
+    if (mode == 1) {
+      H = 1;
+      S = G;
+      size_t fixed = strip_smem_bytes(1, G, 0);
+      ent_cap = (int)((std::min<size_t>(smem_optin ? smem_optin : 232448, 220 * 1024) - fixed) / 17);
+      return;
+    }
+    int best_h = 1;
+    for (int h : {8, 4, 2, 1}) {
+      if (force_h && h != force_h) continue;
+      const size_t fixed = strip_smem_bytes(h, G, 0);
+      if (fixed >= budget) continue;
+      const int cap = (int)((budget - fixed) / 17);
+      if (force_h || cap >= (5 * h * G) / 4) { best_h = h; break; }
+    }
+    H = best_h;
+    S = (G + H - 1) / H;
+    const size_t fixed = strip_smem_bytes(H, G, 0);
+    ent_cap = (int)((budget > fixed ? budget - fixed : 0) / 17);
+  }
+
+  int upload(const float* f32, const int* i32, const float* ypr, const int* tri_h, const float* vtx,
+             const float* vnrm_h)
+  {
+    P = read_params(f32, i32);
+    if (P.n_tri < 0 || P.n_vtx < 0 || P.n_ypr < 0) return set_error(TOMO_ERR_ARG, "negative size in Int32Info");
+    if (P.n_ypr > 0 && ypr == nullptr) return set_error(TOMO_ERR_ARG, "YPR is null");
+    if (P.n_tri > 0 && (tri_h == nullptr || vtx == nullptr || vnrm_h == nullptr))
+      return set_error(TOMO_ERR_ARG, "mesh array is null");
+    for (int t = 0; t < P.n_tri * 3; t++)
+      if (tri_h[t] < 0 || tri_h[t] >= P.n_vtx) return set_error(TOMO_ERR_ARG, "triangle index out of range");
+    for (int k = 0; k < P.n_vtx * 3; k++)
+      if (!std::isfinite(vtx[k]) || !std::isfinite(vnrm_h[k])) return set_error(TOMO_ERR_ARG, "non-finite vertex or normal");
+    for (int k = 0; k < P.n_ypr * 3; k++)
+      if (!std::isfinite(ypr[k])) return set_error(TOMO_ERR_ARG, "non-finite orientation");
+    if (!std::isfinite(P.dVoxel) || !std::isfinite(P.bed_outer) || !std::isfinite(P.theta_c) || P.bed_outer < 0.f ||
+        P.bed_outer > 1000.f)
+      return set_error(TOMO_ERR_ARG, "bad printer parameters");
+    nYPR = P.n_ypr;
+    // AABB centre of the raw vertices (STomoAABB3Df.cpp:58-72)
+    float mn[3] = {1e5f, 1e5f, 1e5f}, mx[3] = {-1e5f, -1e5f, -1e5f};
+    for (int v = 0; v < P.n_vtx; v++)
+      for (int k = 0; k < 3; k++) {
+        const float d = vtx[v * 3 + k];
+        mn[k] = (mn[k] <= d) ? mn[k] : d;
+        mx[k] = (mx[k] >= d) ? mx[k] : d;
+      }
+    cx = (float)((double)(mn[0] + mx[0]) * 0.5);
+    cy = (float)((double)(mn[1] + mx[1]) * 0.5);
+    cz = (float)((double)(mn[2] + mx[2]) * 0.5);
+    G = choose_grid(vtx, P.n_vtx);
+    if (G > kMaxGrid) return set_error(TOMO_ERR_CAPACITY, "mesh extent exceeds the supported slot grid");
+
+    std::vector<float4> hp(std::max(P.n_vtx, 1)), hn(std::max(P.n_vtx, 1));
+    for (int v = 0; v < P.n_vtx; v++) {
+      hp[v] = make_float4(vtx[v * 3 + 0], vtx[v * 3 + 1], vtx[v * 3 + 2], 0.f);
+      hn[v] = make_float4(vnrm_h[v * 3 + 0], vnrm_h[v * 3 + 1], vnrm_h[v * 3 + 2], 0.f);
+    }
+    std::vector<int4> ht(std::max(P.n_tri, 1));
+    for (int t = 0; t < P.n_tri; t++) ht[t] = make_int4(tri_h[t * 3 + 0], tri_h[t * 3 + 1], tri_h[t * 3 + 2], 0);
+    h_rot.assign((size_t)std::max(nYPR, 1) * 9, 0.f);
+    for (int i = 0; i < nYPR; i++) rotation(ypr[i * 3 + 0], ypr[i * 3 + 1], ypr[i * 3 + 2], &h_rot[(size_t)i * 9]);
+    std::vector<int> hori(std::max(nYPR, 1));
+    for (int i = 0; i < nYPR; i++) hori[i] = i;
+
+    TOMO_CUDA(vpos.reserve(hp.size())); TOMO_CUDA(vnrm.reserve(hn.size()));
+    TOMO_CUDA(tri.reserve(ht.size())); TOMO_CUDA(rot.reserve(h_rot.size())); TOMO_CUDA(ori.reserve(hori.size()));
+    TOMO_CUDA(cudaMemcpyAsync(vpos.ptr, hp.data(), sizeof(float4) * hp.size(), cudaMemcpyHostToDevice, main));
+    TOMO_CUDA(cudaMemcpyAsync(vnrm.ptr, hn.data(), sizeof(float4) * hn.size(), cudaMemcpyHostToDevice, main));
+    TOMO_CUDA(cudaMemcpyAsync(tri.ptr, ht.data(), sizeof(int4) * ht.size(), cudaMemcpyHostToDevice, main));
+    TOMO_CUDA(cudaMemcpyAsync(rot.ptr, h_rot.data(), sizeof(float) * h_rot.size(), cudaMemcpyHostToDevice, main));
+    TOMO_CUDA(cudaMemcpyAsync(ori.ptr, hori.data(), sizeof(int) * hori.size(), cudaMemcpyHostToDevice, main));
+    TOMO_CUDA(cudaStreamSynchronize(main));
+    return 0;
+  }
+
+  EngineParams base_params(int mode)
+  {
+    EngineParams p;
+    std::memset(&p, 0, sizeof(p));
+    p.vpos = vpos.ptr; p.vnrm = vnrm.ptr; p.tri = tri.ptr; p.nV = P.n_vtx; p.nT = P.n_tri;
+    p.rot = rot.ptr;
+    p.cx = cx; p.cy = cy; p.cz = cz;
+    p.bed_outer = P.bed_outer; p.bed_inner = P.bed_inner; p.bed_type = P.bed_type;
+    p.bed_r = (int)P.bed_outer; p.bed_thickness = P.bed_thickness;
+    p.G = G; p.H = H; p.S = S; p.mode = mode;
+    p.half = P.dVoxel * 0.5f;
+    p.shell_off = (float)(int)(P.shell_thickness + 0.999f);
+    p.twin = (P.shell && P.shell_thickness > 0.001f) ? 1 : 0;
+    p.vmax = largest_float_not_above(1.0 + (double)0.001f);
+    p.thr = (float)(-1.0 * (double)sinf(P.theta_c));   // STomoSh_INT3.cpp:756
+    p.explicit_ss = P.explicit_ss;
+    p.ent_cap = ent_cap;
+    p.out_vo = o_vo.ptr; p.out_vss = o_vss.ptr; p.out_vtc = o_vtc.ptr;
+    p.out_vof = o_vof.ptr; p.out_vssf = o_vssf.ptr; p.out_vtcf = o_vtcf.ptr;
+    p.out_nbed = o_nbed.ptr; p.out_flags = o_flags.ptr; p.out_entries = o_ent.ptr; p.out_columns = o_col.ptr;
+    p.dump_slot = -1;
+    return p;
+  }
+
+  int reserve_batch(int Bo, int bin_cap)
+  {
+    const size_t GG = (size_t)G * G;
+    TOMO_CUDA(xf.reserve((size_t)Bo * std::max(P.n_vtx, 1)));
+    TOMO_CUDA(minkey.reserve((size_t)Bo * 4));
+    TOMO_CUDA(tcode.reserve((size_t)Bo * std::max(P.n_tri, 1)));
+    TOMO_CUDA(bin_off.reserve((size_t)Bo * (S + 1)));
+    TOMO_CUDA(bin_cur.reserve((size_t)Bo * S));
+    TOMO_CUDA(bins.reserve((size_t)Bo * bin_cap));
+    TOMO_CUDA(bbox.reserve((size_t)Bo * 4));
+    TOMO_CUDA(bedf.reserve((size_t)Bo * GG));
+    for (auto& s : set) {
+      TOMO_CUDA(s.acc.reserve((size_t)Bo * kAccLanes));
+      TOMO_CUDA(s.flags.reserve((size_t)Bo));
+      TOMO_CUDA(s.foldcnt.reserve((size_t)Bo * S));
+      TOMO_CUDA(s.foldv.reserve((size_t)Bo * GG));
+    }
+    return 0;
+  }
+
+  int reserve_outputs()
+  {
+    const size_t n = (size_t)std::max(nYPR, 1);
+    TOMO_CUDA(o_vo.reserve(n)); TOMO_CUDA(o_vss.reserve(n)); TOMO_CUDA(o_vtc.reserve(n));
+    TOMO_CUDA(o_ent.reserve(n)); TOMO_CUDA(o_col.reserve(n));
+    TOMO_CUDA(o_vof.reserve(n)); TOMO_CUDA(o_vssf.reserve(n)); TOMO_CUDA(o_vtcf.reserve(n));
+    TOMO_CUDA(o_nbed.reserve(n)); TOMO_CUDA(o_flags.reserve(n));
+    return 0;
+  }
+
+  void bind_batch(EngineParams& p, int Bo, int bin_cap, int which, int first)
+  {
+    p.Bo = Bo;
+    p.ori = ori.ptr + first;
+    p.xf = xf.ptr; p.minkey = minkey.ptr; p.tcode = tcode.ptr;
+    p.bin_off = bin_off.ptr; p.bin_cur = bin_cur.ptr; p.bins = bins.ptr; p.bin_cap = bin_cap;
+    p.bbox = bbox.ptr; p.bedf = bedf.ptr;
+    p.acc = set[which].acc.ptr; p.flags = set[which].flags.ptr;
+    p.foldcnt = set[which].foldcnt.ptr; p.foldv = set[which].foldv.ptr;
+  }
+
+  // All orientations in normal mode (or safe mode when forced), asynchronously on `main`.
+  int sweep_device()
+  {
+    if (nYPR == 0 || P.n_tri == 0) return 0;
+    const int mode = force_safe ? 1 : 0;
+    choose_strips(mode);
+    const size_t smem = strip_smem_bytes(H, G, ent_cap);
+    TOMO_CUDA(configure_kernels(smem));
+    const int Bo = std::min(batch, nYPR);
+    const int bin_cap = mode == 0 ? 4 * P.n_tri + 4096 : 0;
+    if (mode == 1) return run_safe_all();
+    TOMO_TRY(reserve_outputs());
+    TOMO_TRY(reserve_batch(Bo, bin_cap));
+    TOMO_CUDA(cudaMemsetAsync(o_nbed.ptr, 0, sizeof(int) * nYPR, main));
+    EngineParams p = base_params(0);
+    int k = 0;
+    for (int first = 0; first < nYPR; first += Bo, k++) {
+      const int nb = std::min(Bo, nYPR - first);
+      const int which = k & 1;
+      if (k >= 2) TOMO_CUDA(cudaStreamWaitEvent(main, set[which].folded, 0));
+      bind_batch(p, nb, bin_cap, which, first);
+      TOMO_CUDA(launch_batch(p, main, smem));
+      TOMO_CUDA(cudaEventRecord(ev_ready, main));
+      TOMO_CUDA(cudaStreamWaitEvent(side, ev_ready, 0));
+      TOMO_CUDA(launch_fold(p, side));
+      TOMO_CUDA(cudaEventRecord(set[which].folded, side));
+    }
+    // join the side stream back into main
+    TOMO_CUDA(cudaEventRecord(ev_ready, side));
+    TOMO_CUDA(cudaStreamWaitEvent(main, ev_ready, 0));
+    return 0;
+  }
+
+  // Safe mode for a list of orientation ids (host-synchronous: the bin
+  // buffer is sized from the exact counts).
+  int run_safe(const std::vector<int>& ids)
+  {
+    if (ids.empty()) return 0;
+    choose_strips(1);
+    const size_t smem = strip_smem_bytes(H, G, ent_cap);
+    TOMO_CUDA(configure_kernels(smem));
+    TOMO_TRY(reserve_outputs());
+    DevBuf<int> sub;
+    TOMO_CUDA(sub.reserve(ids.size()));
+    TOMO_CUDA(cudaMemcpyAsync(sub.ptr, ids.data(), sizeof(int) * ids.size(), cudaMemcpyHostToDevice, main));
+    const int Bo = std::min<int>(batch, (int)ids.size());
+    TOMO_TRY(reserve_batch(Bo, 1));
+    EngineParams p = base_params(1);
+    for (int first = 0; first < (int)ids.size(); first += Bo) {
+      const int nb = std::min<int>(Bo, (int)ids.size() - first);
+      // The count pass decides the bin capacity, so it runs without one.
+      bind_batch(p, nb, INT_MAX, 0, 0);
+      p.ori = sub.ptr + first;
+      TOMO_CUDA(launch_bin_count(p, main));
+      std::vector<int> off((size_t)nb * (S + 1));
+      TOMO_CUDA(cudaMemcpyAsync(off.data(), bin_off.ptr, sizeof(int) * off.size(), cudaMemcpyDeviceToHost, main));
+      TOMO_CUDA(cudaStreamSynchronize(main));
+      int cap = 1;
+      for (int o = 0; o < nb; o++) cap = std::max(cap, off[(size_t)o * (S + 1) + S]);
+      TOMO_CUDA(bins.reserve((size_t)nb * cap));
+      p.bins = bins.ptr; p.bin_cap = cap;
+      for (int o = 0; o < nb; o++) TOMO_CUDA(cudaMemsetAsync(o_nbed.ptr + ids[first + o], 0, sizeof(int), main));
+      TOMO_CUDA(launch_after_count(p, main, smem));
+      TOMO_CUDA(launch_fold(p, main));
+      TOMO_CUDA(cudaStreamSynchronize(main));
+    }
+    sub.release();
+    n_safe += (int)ids.size();
+    return 0;
+  }
+
+  int run_safe_all()
+  {
+    std::vector<int> ids(nYPR);
+    for (int i = 0; i < nYPR; i++) ids[i] = i;
+    TOMO_TRY(reserve_outputs());
+    TOMO_CUDA(cudaMemsetAsync(o_nbed.ptr, 0, sizeof(int) * nYPR, main));
+    return run_safe(ids);
+  }
+
+  int fetch()
+  {
+    const size_t n = (size_t)nYPR;
+    vo64.assign(n, 0); vss64.assign(n, 0); vtc64.assign(n, 0); entries.assign(n, 0); columns.assign(n, 0);
+    vof.assign(n, 0.f); vssf.assign(n, 0.f); vtcf.assign(n, 0.f); nbed.assign(n, 0); flags.assign(n, 0);
+    if (n == 0 || P.n_tri == 0) return 0;
+    TOMO_CUDA(cudaMemcpyAsync(vo64.data(), o_vo.ptr, sizeof(long long) * n, cudaMemcpyDeviceToHost, main));
+    TOMO_CUDA(cudaMemcpyAsync(vss64.data(), o_vss.ptr, sizeof(long long) * n, cudaMemcpyDeviceToHost, main));
+    TOMO_CUDA(cudaMemcpyAsync(vtc64.data(), o_vtc.ptr, sizeof(long long) * n, cudaMemcpyDeviceToHost, main));
+    TOMO_CUDA(cudaMemcpyAsync(entries.data(), o_ent.ptr, sizeof(long long) * n, cudaMemcpyDeviceToHost, main));
+    TOMO_CUDA(cudaMemcpyAsync(columns.data(), o_col.ptr, sizeof(long long) * n, cudaMemcpyDeviceToHost, main));
+    TOMO_CUDA(cudaMemcpyAsync(vof.data(), o_vof.ptr, sizeof(float) * n, cudaMemcpyDeviceToHost, main));
+    TOMO_CUDA(cudaMemcpyAsync(vssf.data(), o_vssf.ptr, sizeof(float) * n, cudaMemcpyDeviceToHost, main));
+    TOMO_CUDA(cudaMemcpyAsync(vtcf.data(), o_vtcf.ptr, sizeof(float) * n, cudaMemcpyDeviceToHost, main));
+    TOMO_CUDA(cudaMemcpyAsync(nbed.data(), o_nbed.ptr, sizeof(int) * n, cudaMemcpyDeviceToHost, main));
+    TOMO_CUDA(cudaMemcpyAsync(flags.data(), o_flags.ptr, sizeof(int) * n, cudaMemcpyDeviceToHost, main));
+    TOMO_CUDA(cudaStreamSynchronize(main));
+    return 0;
+  }
+
+  // Full device phase: normal sweep, then safe re-runs of flagged orientations.
+  int execute()
+  {
+    n_safe = 0;
+    int rc = sweep_device();
+    if (rc) return rc;
+    rc = fetch();
+    if (rc) return rc;
+    std::vector<int> redo;
+    for (int i = 0; i < nYPR; i++) {
+      if (flags[i] & kFlagGrid) return set_error(TOMO_ERR_CAPACITY, "slot index outside the grid");
+      if (flags[i] & (kFlagStray | kFlagOverflow | kFlagBinCap)) redo.push_back(i);
+    }
+    if (!redo.empty()) {
+      rc = run_safe(redo);
+      if (rc) return rc;
+      rc = fetch();
+      if (rc) return rc;
+    }
+    for (int i = 0; i < nYPR; i++) {
+      if (flags[i] & kFlagSafeOverflow) return set_error(TOMO_ERR_CAPACITY, "column strip exceeds shared memory");
+      if (flags[i] & kFlagGrid) return set_error(TOMO_ERR_CAPACITY, "slot index outside the grid");
+      if (flags[i] & (kFlagStray | kFlagOverflow | kFlagBinCap))
+        return set_error(TOMO_ERR_CAPACITY, "orientation unresolved after the safe re-run");
+    }
+    return 0;
+  }
+
+  // One orientation with the dense per-column dump enabled (parity tests).
+  int dump(int id, int mode, int* cols8, unsigned* keys64, short* types64)
+  {
+    if (id < 0 || id >= nYPR) return set_error(TOMO_ERR_ARG, "orientation index out of range");
+    if (P.n_tri == 0) return set_error(TOMO_ERR_ARG, "empty mesh");
+    choose_strips(mode);
+    const size_t smem = strip_smem_bytes(H, G, ent_cap);
+    TOMO_CUDA(configure_kernels(smem));
+    TOMO_TRY(reserve_outputs());
+    const size_t GG = (size_t)G * G;
+    TOMO_CUDA(dump_cols.reserve(GG * 8)); TOMO_CUDA(dump_keys.reserve(GG * 64)); TOMO_CUDA(dump_types.reserve(GG * 64));
+    TOMO_CUDA(cudaMemsetAsync(dump_cols.ptr, 0, sizeof(int) * GG * 8, main));
+    TOMO_CUDA(cudaMemsetAsync(dump_keys.ptr, 0, sizeof(unsigned) * GG * 64, main));
+    TOMO_CUDA(cudaMemsetAsync(dump_types.ptr, 0, sizeof(short) * GG * 64, main));
+    TOMO_CUDA(cudaMemsetAsync(o_nbed.ptr + id, 0, sizeof(int), main));
+    EngineParams p = base_params(mode);
+    p.dump_slot = 0; p.dump_cols = dump_cols.ptr; p.dump_keys = dump_keys.ptr; p.dump_types = dump_types.ptr;
+    int cap = 4 * P.n_tri + 4096;
+    TOMO_TRY(reserve_batch(1, mode == 0 ? cap : 1));
+    bind_batch(p, 1, mode == 0 ? cap : INT_MAX, 0, id);
+    if (mode == 0) {
+      TOMO_CUDA(launch_batch(p, main, smem));
+    } else {
+      TOMO_CUDA(launch_bin_count(p, main));
+      int total = 0;
+      TOMO_CUDA(cudaMemcpyAsync(&total, bin_off.ptr + S, sizeof(int), cudaMemcpyDeviceToHost, main));
+      TOMO_CUDA(cudaStreamSynchronize(main));
+      cap = std::max(total, 1);
+      TOMO_CUDA(bins.reserve((size_t)cap));
+      p.bins = bins.ptr; p.bin_cap = cap;
+      TOMO_CUDA(launch_after_count(p, main, smem));
+    }
+    TOMO_CUDA(launch_fold(p, main));
+    if (cols8) TOMO_CUDA(cudaMemcpyAsync(cols8, dump_cols.ptr, sizeof(int) * GG * 8, cudaMemcpyDeviceToHost, main));
+    if (keys64) TOMO_CUDA(cudaMemcpyAsync(keys64, dump_keys.ptr, sizeof(unsigned) * GG * 64, cudaMemcpyDeviceToHost, main));
+    if (types64) TOMO_CUDA(cudaMemcpyAsync(types64, dump_types.ptr, sizeof(short) * GG * 64, cudaMemcpyDeviceToHost, main));
+    TOMO_CUDA(cudaStreamSynchronize(main));
+    int fl = 0;
+    TOMO_CUDA(cudaMemcpy(&fl, o_flags.ptr + id, sizeof(int), cudaMemcpyDeviceToHost));
+    return fl;
+  }
+
+  // Float fold of n additions of BedThickness: Calculate adds
+  // sumType(typeBed) * BedThickness per bed slot (STomoSh_INT3.cpp:1240), and
+  // every bed slot holds exactly one bed pixel at z = 1.
+  void finalize_host()
+  {
+    const size_t n = (size_t)nYPR;
+    Mo.assign(n + 2, 0.f); Mss.assign(n + 2, 0.f); Vtc.assign(n + 2, 0.f);
+    int maxbed = 0;
+    for (size_t i = 0; i < n; i++) maxbed = std::max(maxbed, nbed[i]);
+    std::vector<float> bedfold((size_t)maxbed + 1, 0.f);
+    for (int k = 1; k <= maxbed; k++) bedfold[k] = bedfold[k - 1] + (float)1 * P.bed_thickness;
+    for (size_t i = 0; i < n; i++) {
+      float vm[22] = {0};
+      vm[8] = vof[i];
+      vm[4] = vssf[i];
+      vm[2] = vtcf[i];
+      vm[11] = bedfold[nbed[i]];
+      vol_to_mass(P, vm);
+      Mo[i] = vm[16];
+      Mss[i] = vm[13];
+      Vtc[i] = vm[2];
+    }
+  }
+};
+
+namespace {
+Engine* g_engine = nullptr;
+std::vector<float> g_Mss, g_Mo, g_Vtc;
+std::vector<long long> g_Vo64, g_Vss64, g_Vtc64;
+float g_volmass[22] = {0};
+float g_mat4x4[16] = {0};
+std::vector<short> g_pix[11];
+int g_npix[11] = {0};
+
+Engine& engine()
+{
+  if (!g_engine) g_engine = new Engine();
+  return *g_engine;
+}
+
+// mat4x4 of STomoSh_Base::Rotate (STomoSh_Base.cpp:155-167) for one orientation.
+void host_mat4x4(const Engine& E, const float* vtx, int nV, int id, float* m16)
+{
+  const float* R = &E.h_rot[(size_t)id * 9];
+  float mn[3] = {1e5f, 1e5f, 1e5f};
+  for (int v = 0; v < nV; v++) {
+    const float t0 = vtx[v * 3 + 0] - E.cx, t1 = vtx[v * 3 + 1] - E.cy, t2 = vtx[v * 3 + 2] - E.cz;
+    for (int r = 0; r < 3; r++) {
+      float s = R[r * 3 + 0] * t0;
+      s += R[r * 3 + 1] * t1;
+      s += R[r * 3 + 2] * t2;
+      s += 0.0f * 1.0f;
+      mn[r] = (mn[r] <= s) ? mn[r] : s;
+    }
+  }
+  const float dx = mn[0] - E.P.bed_outer, dy = mn[1] - E.P.bed_outer, dz = mn[2];
+  const float m = -E.cx, n = -E.cy, o = -E.cz;
+  std::memset(m16, 0, 16 * sizeof(float));
+  for (int r = 0; r < 3; r++)
+    for (int k = 0; k < 3; k++) m16[r * 4 + k] = R[r * 3 + k];
+  m16[15] = 1.f;
+  m16[3] = -dx + R[0] * m + R[1] * n + R[2] * o;
+  m16[7] = -dy + R[3] * m + R[4] * n + R[5] * o;
+  m16[11] = -dz + R[6] * m + R[7] * n + R[8] * o;
+}
+}  // namespace
+
+}  // namespace tomo
+
+using namespace tomo;
+
+// ------------------------------------------------ C-ABI
+
+extern "C" {
+
+int TomoSh_CUDA(float* f32info, int* i32info, float* YPR, int* tri, float* vtx, float* vtx_nrm, float* tri_nrm,
+                int* chull_tri, float* chull_vtx, float* chull_trinrm)
+{
+  (void)tri_nrm; (void)chull_tri; (void)chull_vtx; (void)chull_trinrm;
+  std::lock_guard<std::mutex> lock(g_mutex);
+  g_last_error = 0; g_last_error_str.clear();
+  if (f32info == nullptr || i32info == nullptr) return set_error(TOMO_ERR_ARG, "info arrays are null");
+  Engine& E = engine();
+  int rc = E.init();
+  if (rc) return rc;
+  rc = E.upload(f32info, i32info, YPR, tri, vtx, vtx_nrm);
+  if (rc) return rc;
+  rc = E.execute();
+  if (rc) return rc;
+  E.finalize_host();
+  const int n = E.nYPR;
+  g_Mss.assign(E.Mss.begin(), E.Mss.end());
+  g_Mo.assign(E.Mo.begin(), E.Mo.end());
+  g_Vtc.assign(E.Vtc.begin(), E.Vtc.end());
+  g_Vo64 = E.vo64; g_Vss64 = E.vss64; g_Vtc64 = E.vtc64;
+  const int opt = first_optimal(n, g_Mss.data());
+  std::memset(g_volmass, 0, sizeof(g_volmass));
+  if (n > 0) {
+    g_volmass[8] = E.vof[opt]; g_volmass[4] = E.vssf[opt]; g_volmass[2] = E.vtcf[opt];
+    vol_to_mass(E.P, g_volmass);
+    host_mat4x4(E, vtx, E.P.n_vtx, opt, g_mat4x4);
+  }
+  for (int k = 0; k < 11; k++) { g_pix[k].clear(); g_npix[k] = 0; }
+  return opt;
+}
+
+float* getMss(void) { return g_Mss.empty() ? nullptr : g_Mss.data(); }
+float* getMo(void) { return g_Mo.empty() ? nullptr : g_Mo.data(); }
+float* getVtc(void) { return g_Vtc.empty() ? nullptr : g_Vtc.data(); }
+float* getVolMassInfo(void) { return g_volmass; }
+float* getMat4x4(void) { return g_mat4x4; }
+int getnData2i(short type) { return (type >= 0 && type < 11) ? g_npix[type] : 0; }
+short* getpData2i(short type)
+{
+  if (type < 0 || type >= 11 || g_pix[type].empty()) return nullptr;
+  return g_pix[type].data();
+}
+const long long* getVo64(void) { return g_Vo64.empty() ? nullptr : g_Vo64.data(); }
+const long long* getVss64(void) { return g_Vss64.empty() ? nullptr : g_Vss64.data(); }
+const long long* getVtc64(void) { return g_Vtc64.empty() ? nullptr : g_Vtc64.data(); }
+
+void OnDestroy(void)
+{
+  std::lock_guard<std::mutex> lock(g_mutex);
+  g_Mss.clear(); g_Mo.clear(); g_Vtc.clear(); g_Vo64.clear(); g_Vss64.clear(); g_Vtc64.clear();
+  g_Mss.shrink_to_fit(); g_Mo.shrink_to_fit(); g_Vtc.shrink_to_fit();
+  for (auto& v : g_pix) { v.clear(); v.shrink_to_fit(); }
+  std::memset(g_npix, 0, sizeof(g_npix));
+  if (g_engine) { g_engine->release(); delete g_engine; g_engine = nullptr; }
+}
+
+int tomoGetLastError(void) { return g_last_error; }
+const char* tomoGetLastErrorString(void) { return g_last_error_str.c_str(); }
+
+void tomoRotation(float yaw, float pitch, float roll, float* out9) { rotation(yaw, pitch, roll, out9); }
+
+float tomoShadowThreshold(float theta_c) { return (float)(-1.0 * (double)sinf(theta_c)); }
+
+void tomoVolToMass(const float* f32info, const int* i32info, float* vm22)
+{
+  vol_to_mass(read_params(f32info, i32info), vm22);
+}
+
+int tomoSetOption(int key, int value)
+{
+  std::lock_guard<std::mutex> lock(g_mutex);
+  Engine& E = engine();
+  switch (key) {
+    case TOMO_OPT_BATCH: if (value < 1) return TOMO_ERR_ARG; E.batch = value; return 0;
+    case TOMO_OPT_STRIP_H: if (value < 0 || value > 8) return TOMO_ERR_ARG; E.force_h = value; return 0;
+    case TOMO_OPT_FORCE_SAFE: E.force_safe = value ? 1 : 0; return 0;
+    default: return TOMO_ERR_ARG;
+  }
+}
+
+int tomoGetStats(long long* out, int n)
+{
+  std::lock_guard<std::mutex> lock(g_mutex);
+  if (!g_engine || out == nullptr) return TOMO_ERR_ARG;
+  const Engine& E = *g_engine;
+  const long long v[8] = {E.G, E.H, E.S, E.ent_cap, E.n_safe, E.nYPR, E.batch, 0};
+  for (int i = 0; i < n && i < 8; i++) out[i] = v[i];
+  return 0;
+}
+
+// Per-orientation exact results of the last TomoSh_CUDA / tomoSweep call.
+int tomoGetResults(long long* vo64, long long* vss64, long long* vtc64, float* vof, float* vssf, float* vtcf,
+                   int* nbed, int* flags, long long* entries, long long* columns)
+{
+  std::lock_guard<std::mutex> lock(g_mutex);
+  if (!g_engine) return TOMO_ERR_ARG;
+  const Engine& E = *g_engine;
+  const size_t n = (size_t)E.nYPR;
+  if (vo64) std::memcpy(vo64, E.vo64.data(), sizeof(long long) * n);
+  if (vss64) std::memcpy(vss64, E.vss64.data(), sizeof(long long) * n);
+  if (vtc64) std::memcpy(vtc64, E.vtc64.data(), sizeof(long long) * n);
+  if (vof) std::memcpy(vof, E.vof.data(), sizeof(float) * n);
+  if (vssf) std::memcpy(vssf, E.vssf.data(), sizeof(float) * n);
+  if (vtcf) std::memcpy(vtcf, E.vtcf.data(), sizeof(float) * n);
+  if (nbed) std::memcpy(nbed, E.nbed.data(), sizeof(int) * n);
+  if (flags) std::memcpy(flags, E.flags.data(), sizeof(int) * n);
+  if (entries) std::memcpy(entries, E.entries.data(), sizeof(long long) * n);
+  if (columns) std::memcpy(columns, E.columns.data(), sizeof(long long) * n);
+  return 0;
+}
+
+// Split entry points: upload once, run the device sweep repeatedly (inputs
+// resident in HBM), then fetch.  The sweep runs on the engine's own streams;
+// tomoSweepDevice records cudaEvents around its work when given non-null
+// events (created by the caller) and returns after the device finished.
+int tomoPrepare(const float* f32info, const int* i32info, const float* YPR, const int* tri, const float* vtx,
+                const float* vtx_nrm)
+{
+  std::lock_guard<std::mutex> lock(g_mutex);
+  g_last_error = 0; g_last_error_str.clear();
+  Engine& E = engine();
+  int rc = E.init();
+  if (rc) return rc;
+  return E.upload(f32info, i32info, YPR, tri, vtx, vtx_nrm);
+}
+
+int tomoSweepDevice(void* ev_start, void* ev_stop, float* kernel_ms)
+{
+  std::lock_guard<std::mutex> lock(g_mutex);
+  if (!g_engine || !g_engine->main) return set_error(TOMO_ERR_ARG, "tomoPrepare was not called");
+  Engine& E = *g_engine;
+  cudaEvent_t a = (cudaEvent_t)ev_start, b = (cudaEvent_t)ev_stop;
+  cudaEvent_t la = nullptr, lb = nullptr;
+  if (!a) { TOMO_CUDA(cudaEventCreate(&la)); a = la; }
+  if (!b) { TOMO_CUDA(cudaEventCreate(&lb)); b = lb; }
+  TOMO_CUDA(cudaEventRecord(a, E.main));
+  int rc = E.execute();
+  if (rc == 0) {
+    TOMO_CUDA(cudaEventRecord(b, E.main));
+    TOMO_CUDA(cudaEventSynchronize(b));
+    float ms = 0.f;
+    TOMO_CUDA(cudaEventElapsedTime(&ms, a, b));
+    E.last_kernel_ms = ms;
+    if (kernel_ms) *kernel_ms = ms;
+  }
+  if (la) cudaEventDestroy(la);
+  if (lb) cudaEventDestroy(lb);
+  return rc;
+}
+
+int tomoGridSize(void)
+{
+  std::lock_guard<std::mutex> lock(g_mutex);
+  return g_engine ? g_engine->G : 0;
+}
+
+int tomoColumnDump(int ypr_index, int safe_mode, int* cols8, unsigned* keys64, short* types64)
+{
+  std::lock_guard<std::mutex> lock(g_mutex);
+  if (!g_engine || !g_engine->main) return set_error(TOMO_ERR_ARG, "tomoPrepare was not called");
+  return g_engine->dump(ypr_index, safe_mode ? 1 : 0, cols8, keys64, types64);
+}
+
+int tomoFinish(float* Mo, float* Mss, float* Vtc)
+{
+  std::lock_guard<std::mutex> lock(g_mutex);
+  if (!g_engine) return set_error(TOMO_ERR_ARG, "tomoPrepare was not called");
+  Engine& E = *g_engine;
+  E.finalize_host();
+  const size_t n = (size_t)E.nYPR;
+  if (Mo) std::memcpy(Mo, E.Mo.data(), sizeof(float) * n);
+  if (Mss) std::memcpy(Mss, E.Mss.data(), sizeof(float) * n);
+  if (Vtc) std::memcpy(Vtc, E.Vtc.data(), sizeof(float) * n);
+  return first_optimal((int)n, E.Mss.data());
+}
+
+}  // extern "C"

@@ -1,0 +1,1017 @@
+// B200 kernels of the orientation search (sm_100a).
+//
+// One batch of orientations runs as
+//   k_reset -> k_rotate -> k_bin_count -> k_bin_scan -> k_bin_fill -> k_strip
+//   -> k_bed, and k_fold on a second stream;
+// see the launch sequence in tomo_engine.cpp.  The work per orientation is the
+// reference INT3 pipeline (Tomo_Shell2026.cpp thread_func:138-156):
+// Rotate -> Pixelize -> Pairing -> GenerateBed -> Calculate, re-organised so
+// that the per-column pixel lists never leave shared memory:
+//
+//  * the slot grid is cut into strips of H x-columns; triangles are binned
+//    per (orientation, strip) by their pixel bounding box (k_bin_*);
+//  * one CTA per (orientation, strip) rasterizes its triangles into
+//    per-column linked lists in shared memory, then runs the column stage
+//    (dedup, 63-pixel cap, sort, brief pairing, shadow casting) per column,
+//    reduces the column volumes to int64 and writes the non-zero column
+//    values in slot order for the float32 fold (k_strip);
+//  * the rare cases that a strip cannot resolve alone -- a hit whose slot
+//    lands in another strip, or a strip whose lists overflow shared memory --
+//    flag the orientation, which the host re-runs in "safe" mode (H = 1,
+//    every triangle pixel evaluated by every strip its extended box touches).
+//
+// No kernel waits on another CTA; every shared and global index is checked.
+#include "tomo_common.cuh"
+
+#include <climits>
+
+namespace tomo {
+
+// ---------------------------------------------------------------- helpers
+
+__device__ __forceinline__ unsigned f2key(float f)
+{
+  const unsigned b = __float_as_uint(f);
+  return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+
+__device__ __forceinline__ float key2f(unsigned k)
+{
+  return __uint_as_float((k & 0x80000000u) ? (k & 0x7FFFFFFFu) : ~k);
+}
+
+// _min/_max of Tomo_types.cpp:30-46
+__device__ __forceinline__ float fmin_ref(float a, float b) { return (a <= b) ? a : b; }
+__device__ __forceinline__ float fmax_ref(float a, float b) { return (a >= b) ? a : b; }
+
+// SMatrix4f::Dot row (SMatrix4f.cpp:242-262): sequential +=, then + Data[i][3]*1 (= 0).
+__device__ __forceinline__ float row_dot(float r0, float r1, float r2, float t0, float t1, float t2)
+{
+  float s = __fmul_rn(r0, t0);
+  s = __fadd_rn(s, __fmul_rn(r1, t1));
+  s = __fadd_rn(s, __fmul_rn(r2, t2));
+  return __fadd_rn(s, 0.0f);
+}
+
+// _dot of two (x, y, 0) vectors (Tomo_types.cpp:14-17).
+__device__ __forceinline__ float dot2(float ax, float ay, float bx, float by)
+{
+  return __fadd_rn(__fadd_rn(__fmul_rn(ax, bx), __fmul_rn(ay, by)), 0.0f);
+}
+
+// _bary_product (Tomo_types.cpp:75-84): p0*u + p1*v + p2*w, left to right.
+__device__ __forceinline__ float bary3(float p0, float p1, float p2, float u, float v, float w)
+{
+  return __fadd_rn(__fadd_rn(__fmul_rn(p0, u), __fmul_rn(p1, v)), __fmul_rn(p2, w));
+}
+
+__device__ __forceinline__ unsigned make_key(int z, int nz)
+{
+  return ((unsigned)(z + 32768) << 16) | (unsigned)(nz + 32768);
+}
+__device__ __forceinline__ int key_z(unsigned k) { return (int)(k >> 16) - 32768; }
+__device__ __forceinline__ int key_nz(unsigned k) { return (int)(k & 0xFFFFu) - 32768; }
+
+// float -> int16 the way SetBit stores z and nz (STomoVoxelSpaceInfo.cpp:179-180).
+__device__ __forceinline__ int to_i16(float f) { return (int)(short)__float2int_rz(f); }
+
+struct TriGeo {
+  float ax, ay, az, bx, by, bz, cx, cy, cz;  // translated + margined vertices
+  float n0, n1, n2;                          // rotated vertex-normal z
+  int x0, x1, y0, y1;                        // pixel box (STomoSh_INT3.cpp:1156-1159)
+};
+
+struct Shift { float dx, dy, dz; };
+
+__device__ __forceinline__ Shift load_shift(const EngineParams& p, int o)
+{
+  // translation of STomoSh_Base::Rotate (STomoSh_Base.cpp:147-153)
+  Shift s;
+  s.dx = __fsub_rn(key2f(p.minkey[o * 4 + 0]), p.bed_outer);
+  s.dy = __fsub_rn(key2f(p.minkey[o * 4 + 1]), p.bed_outer);
+  s.dz = key2f(p.minkey[o * 4 + 2]);
+  return s;
+}
+
+__device__ __forceinline__ void load_tri(const EngineParams& p, int o, int t, const Shift& sh, TriGeo& g,
+                                         float4* raw = nullptr)
+{
+  const int4 ix = p.tri[t];
+  const float4* X = p.xf + (size_t)o * p.nV;
+  const float4 A = X[ix.x], B = X[ix.y], C = X[ix.z];
+  if (raw) { raw[0] = A; raw[1] = B; raw[2] = C; }
+  g.ax = __fadd_rn(__fsub_rn(A.x, sh.dx), 0.001f);
+  g.ay = __fadd_rn(__fsub_rn(A.y, sh.dy), 0.001f);
+  g.az = __fadd_rn(__fsub_rn(A.z, sh.dz), 0.001f);
+  g.bx = __fadd_rn(__fsub_rn(B.x, sh.dx), 0.001f);
+  g.by = __fadd_rn(__fsub_rn(B.y, sh.dy), 0.001f);
+  g.bz = __fadd_rn(__fsub_rn(B.z, sh.dz), 0.001f);
+  g.cx = __fadd_rn(__fsub_rn(C.x, sh.dx), 0.001f);
+  g.cy = __fadd_rn(__fsub_rn(C.y, sh.dy), 0.001f);
+  g.cz = __fadd_rn(__fsub_rn(C.z, sh.dz), 0.001f);
+  g.n0 = A.w; g.n1 = B.w; g.n2 = C.w;
+  g.x0 = __float2int_rz(fmin_ref(fmin_ref(g.ax, g.bx), g.cx));
+  g.y0 = __float2int_rz(fmin_ref(fmin_ref(g.ay, g.by), g.cy));
+  g.x1 = __float2int_rz(fmax_ref(fmax_ref(g.ax, g.bx), g.cx));
+  g.y1 = __float2int_rz(fmax_ref(fmax_ref(g.ay, g.by), g.cy));
+}
+
+struct Bary { float e0x, e0y, e1x, e1y, d00, d01, d11, denom; bool ok; };
+
+// Triangle-constant part of _getBaryCoord (Tomo_types.cpp:86-101).
+__device__ __forceinline__ void bary_setup(const TriGeo& g, Bary& b)
+{
+  b.e0x = __fsub_rn(g.bx, g.ax); b.e0y = __fsub_rn(g.by, g.ay);
+  b.e1x = __fsub_rn(g.cx, g.ax); b.e1y = __fsub_rn(g.cy, g.ay);
+  b.d00 = dot2(b.e0x, b.e0y, b.e0x, b.e0y);
+  b.d01 = dot2(b.e0x, b.e0y, b.e1x, b.e1y);
+  b.d11 = dot2(b.e1x, b.e1y, b.e1x, b.e1y);
+  b.denom = __fsub_rn(__fmul_rn(b.d00, b.d11), __fmul_rn(b.d01, b.d01));
+  const float ad = (b.denom >= 0.0f) ? b.denom : -b.denom;
+  b.ok = ad > 0.001f;
+}
+
+// Pixel part of _getBaryCoord (Tomo_types.cpp:95-112).  u is formed in
+// double like the reference; the two upper bounds compare against vmax, the
+// largest float not above 1.0 + (double)0.001f, which is the same test.
+__device__ __forceinline__ bool bary_test(float ax, float ay, const Bary& b, float px, float py, float vmax,
+                                          float& u, float& v, float& w)
+{
+  const float e2x = __fsub_rn(px, ax), e2y = __fsub_rn(py, ay);
+  const float d20 = dot2(e2x, e2y, b.e0x, b.e0y);
+  const float d21 = dot2(e2x, e2y, b.e1x, b.e1y);
+  v = __fdiv_rn(__fsub_rn(__fmul_rn(b.d11, d20), __fmul_rn(b.d01, d21)), b.denom);
+  w = __fdiv_rn(__fsub_rn(__fmul_rn(b.d00, d21), __fmul_rn(b.d01, d20)), b.denom);
+  u = __double2float_rn(__dsub_rn(__dsub_rn(1.0, (double)v), (double)w));
+  return (u >= -0.001f) && (v >= -0.001f) && (v <= vmax) && (__fadd_rn(u, v) <= vmax);
+}
+
+// pixel centre (STomoSh_INT3.cpp:1168,1171)
+__device__ __forceinline__ float pix_center(int x, float half) { return __fadd_rn(__fadd_rn((float)x, 0.001f), half); }
+
+// centroid fallback position of a triangle with no pixel hit (STomoSh_INT3.cpp:1190-1206)
+__device__ __forceinline__ float centroid(float a, float b, float c)
+{
+  return __fadd_rn(__fmul_rn(__fadd_rn(__fadd_rn(a, b), c), 0.333333f), 0.001f);
+}
+
+__device__ bool any_hit(const EngineParams& p, const TriGeo& g, const Bary& b)
+{
+  if (!b.ok) return false;
+  for (int x = g.x0; x <= g.x1; x++) {
+    const float px = pix_center(x, p.half);
+    for (int y = g.y0; y <= g.y1; y++) {
+      float u, v, w;
+      if (bary_test(g.ax, g.ay, b, px, pix_center(y, p.half), p.vmax, u, v, w)) return true;
+    }
+  }
+  return false;
+}
+
+// Slot x of the centroid fallback pixel.
+__device__ __forceinline__ int centroid_slot_x(const float4* raw, const Shift& sh)
+{
+  const float ux = centroid(__fsub_rn(raw[0].x, sh.dx), __fsub_rn(raw[1].x, sh.dx), __fsub_rn(raw[2].x, sh.dx));
+  return __float2int_rz(ux);
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v)
+{
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+  return v;
+}
+
+// Block-wide exclusive scan of one int per thread (blockDim.x == 256).
+__device__ __forceinline__ int block_excl_scan(int v, int* warp_tot, int& total)
+{
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  int x = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) warp_tot[wid] = x;
+  __syncthreads();
+  if (wid == 0) {
+    int t = (lane < nw) ? warp_tot[lane] : 0;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xFFFFFFFFu, t, o);
+      if (lane >= o) t += y;
+    }
+    if (lane < nw) warp_tot[lane] = t;
+  }
+  __syncthreads();
+  const int before = (wid > 0) ? warp_tot[wid - 1] : 0;
+  total = warp_tot[nw - 1];
+  __syncthreads();
+  return before + x - v;
+}
+
+// ---------------------------------------------------------------- K0 reset
+
+__global__ void k_reset(EngineParams p)
+{
+  const int o = blockIdx.x;
+  if (threadIdx.x < kAccLanes) p.acc[(size_t)o * kAccLanes + threadIdx.x] = 0;
+  if (threadIdx.x == 0) {
+    p.flags[o] = 0;
+    p.bbox[o * 4 + 0] = INT_MAX; p.bbox[o * 4 + 1] = INT_MAX;
+    p.bbox[o * 4 + 2] = -1; p.bbox[o * 4 + 3] = -1;
+  }
+  if (threadIdx.x < 4) p.minkey[o * 4 + threadIdx.x] = f2key(1e5f);  // STomoAABB3Df::Init
+  for (int s = threadIdx.x; s <= p.S; s += blockDim.x) p.bin_off[(size_t)o * (p.S + 1) + s] = 0;
+  for (int s = threadIdx.x; s < p.S; s += blockDim.x) { p.bin_cur[(size_t)o * p.S + s] = 0; p.foldcnt[(size_t)o * p.S + s] = 0; }
+}
+
+// ---------------------------------------------------------------- K1 rotate
+// STomoSh_Base::Rotate (STomoSh_Base.cpp:45-129): centre on the raw AABB,
+// rotate positions and vertex normals; the AABB minimum of the rotated
+// positions (used for the translation) is reduced with order-preserving
+// atomics.  Only the normal's z component is kept: it is the only one the
+// INT3 path reads (SetBit uses nrm[2]).
+
+__global__ void __launch_bounds__(256) k_rotate(EngineParams p)
+{
+  const int o = blockIdx.y;
+  const float* R = p.rot + (size_t)p.ori[o] * 9;
+  const float r00 = R[0], r01 = R[1], r02 = R[2], r10 = R[3], r11 = R[4], r12 = R[5];
+  const float r20 = R[6], r21 = R[7], r22 = R[8];
+  float mx = 1e5f, my = 1e5f, mz = 1e5f;
+  float4* out = p.xf + (size_t)o * p.nV;
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < p.nV; v += gridDim.x * blockDim.x) {
+    const float4 a = p.vpos[v];
+    const float4 n = p.vnrm[v];
+    const float t0 = __fsub_rn(a.x, p.cx), t1 = __fsub_rn(a.y, p.cy), t2 = __fsub_rn(a.z, p.cz);
+    const float x = row_dot(r00, r01, r02, t0, t1, t2);
+    const float y = row_dot(r10, r11, r12, t0, t1, t2);
+    const float z = row_dot(r20, r21, r22, t0, t1, t2);
+    const float nz = row_dot(r20, r21, r22, n.x, n.y, n.z);
+    out[v] = make_float4(x, y, z, nz);
+    mx = fmin_ref(mx, x); my = fmin_ref(my, y); mz = fmin_ref(mz, z);
+  }
+  for (int off = 16; off > 0; off >>= 1) {
+    mx = fmin_ref(mx, __shfl_xor_sync(0xFFFFFFFFu, mx, off));
+    my = fmin_ref(my, __shfl_xor_sync(0xFFFFFFFFu, my, off));
+    mz = fmin_ref(mz, __shfl_xor_sync(0xFFFFFFFFu, mz, off));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMin(&p.minkey[o * 4 + 0], f2key(mx));
+    atomicMin(&p.minkey[o * 4 + 1], f2key(my));
+    atomicMin(&p.minkey[o * 4 + 2], f2key(mz));
+  }
+}
+
+// ---------------------------------------------------------------- K2 binning
+// Strip range of one triangle.  Normal mode: the strips its pixel box
+// covers; a triangle spanning several strips whose box holds no accepted
+// pixel centre goes only to the strip of its centroid pixel, flagged as
+// "fallback only" (code 2).  Safe mode: the box widened by e columns on both
+// sides, since in safe mode a strip evaluates every pixel of every triangle
+// whose hits could reach it.
+
+struct BinRange { int s0, s1, code; };
+
+__device__ __forceinline__ BinRange bin_range(const EngineParams& p, int o, int t, const Shift& sh, int* flag,
+                                              const uint8_t* known_code)
+{
+  TriGeo g;
+  float4 raw[3];
+  load_tri(p, o, t, sh, g, raw);
+  BinRange r;
+  r.code = 0;
+  if (p.mode == 0) {
+    const int x0 = max(g.x0, 0), x1 = g.x1;
+    if (x1 >= p.G) atomicOr(flag, kFlagGrid);
+    r.s0 = min(x0 / p.H, p.S - 1);
+    r.s1 = min(max(x1, 0) / p.H, p.S - 1);
+    if (r.s0 != r.s1) {
+      int code;
+      if (known_code) code = *known_code;
+      else {
+        Bary b;
+        bary_setup(g, b);
+        code = any_hit(p, g, b) ? 1 : 2;
+      }
+      r.code = code;
+      if (code == 2) {
+        const int cxs = centroid_slot_x(raw, sh);
+        const int sc = min(max(cxs, 0), p.G - 1) / p.H;
+        r.s0 = r.s1 = min(sc, p.S - 1);
+      }
+    }
+  } else {
+    const float xmin = fmin_ref(fmin_ref(g.ax, g.bx), g.cx);
+    const float xmax = fmax_ref(fmax_ref(g.ax, g.bx), g.cx);
+    const int e = 2 + (int)(0.004f * (xmax - xmin));
+    const int lo = max(g.x0 - e, 0);
+    const int hi = min(g.x1 + e, p.G - 1);
+    if (g.x1 >= p.G) atomicOr(flag, kFlagGrid);
+    r.s0 = min(lo / p.H, p.S - 1);
+    r.s1 = min(max(hi, 0) / p.H, p.S - 1);
+  }
+  return r;
+}
+
+__global__ void __launch_bounds__(256) k_bin_count(EngineParams p)
+{
+  extern __shared__ int sh_cnt[];
+  __shared__ int sflag;
+  const int o = blockIdx.y;
+  for (int s = threadIdx.x; s < p.S; s += blockDim.x) sh_cnt[s] = 0;
+  if (threadIdx.x == 0) sflag = 0;
+  __syncthreads();
+  const Shift sh = load_shift(p, o);
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < p.nT; t += gridDim.x * blockDim.x) {
+    const BinRange r = bin_range(p, o, t, sh, &sflag, nullptr);
+    p.tcode[(size_t)o * p.nT + t] = (uint8_t)r.code;
+    for (int s = r.s0; s <= r.s1; s++) atomicAdd(&sh_cnt[s], 1);
+  }
+  __syncthreads();
+  for (int s = threadIdx.x; s < p.S; s += blockDim.x)
+    if (sh_cnt[s]) atomicAdd(&p.bin_off[(size_t)o * (p.S + 1) + s], sh_cnt[s]);
+  if (threadIdx.x == 0 && sflag) atomicOr(&p.flags[o], sflag);
+}
+
+// Exclusive scan of the strip counts of one orientation (one CTA, 1024 threads).
+__global__ void __launch_bounds__(1024) k_bin_scan(EngineParams p)
+{
+  __shared__ int wt[32];
+  const int o = blockIdx.x;
+  int* cnt = p.bin_off + (size_t)o * (p.S + 1);
+  const int per = (p.S + blockDim.x - 1) / blockDim.x;
+  const int b = threadIdx.x * per;
+  int local = 0;
+  for (int i = 0; i < per; i++) if (b + i < p.S) local += cnt[b + i];
+  // block scan (1024 threads = 32 warps)
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  int x = local;
+  for (int off = 1; off < 32; off <<= 1) { const int y = __shfl_up_sync(0xFFFFFFFFu, x, off); if (lane >= off) x += y; }
+  if (lane == 31) wt[wid] = x;
+  __syncthreads();
+  if (wid == 0) {
+    int t = wt[lane];
+    for (int off = 1; off < 32; off <<= 1) { const int y = __shfl_up_sync(0xFFFFFFFFu, t, off); if (lane >= off) t += y; }
+    wt[lane] = t;
+  }
+  __syncthreads();
+  int run = ((wid > 0) ? wt[wid - 1] : 0) + x - local;
+  const int total = wt[31];
+  __syncthreads();
+  for (int i = 0; i < per; i++) {
+    if (b + i < p.S) { const int c = cnt[b + i]; cnt[b + i] = run; run += c; }
+  }
+  if (threadIdx.x == 0) {
+    cnt[p.S] = total;
+    if (total > p.bin_cap) atomicOr(&p.flags[o], kFlagBinCap);
+  }
+}
+
+__global__ void __launch_bounds__(256) k_bin_fill(EngineParams p)
+{
+  extern __shared__ int sh_fill[];
+  int* lc = sh_fill;            // [S]
+  int* base = sh_fill + p.S;    // [S]
+  __shared__ int sflag;
+  const int o = blockIdx.y;
+  for (int s = threadIdx.x; s < p.S; s += blockDim.x) lc[s] = 0;
+  if (threadIdx.x == 0) sflag = 0;
+  __syncthreads();
+  const Shift sh = load_shift(p, o);
+  const int stride = gridDim.x * blockDim.x;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < p.nT; t += stride) {
+    const uint8_t code = p.tcode[(size_t)o * p.nT + t];
+    const BinRange r = bin_range(p, o, t, sh, &sflag, &code);
+    for (int s = r.s0; s <= r.s1; s++) atomicAdd(&lc[s], 1);
+  }
+  __syncthreads();
+  for (int s = threadIdx.x; s < p.S; s += blockDim.x) {
+    base[s] = lc[s] ? atomicAdd(&p.bin_cur[(size_t)o * p.S + s], lc[s]) : 0;
+    lc[s] = 0;
+  }
+  __syncthreads();
+  const int* off = p.bin_off + (size_t)o * (p.S + 1);
+  int* bins = p.bins + (size_t)o * p.bin_cap;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < p.nT; t += stride) {
+    const uint8_t code = p.tcode[(size_t)o * p.nT + t];
+    const BinRange r = bin_range(p, o, t, sh, &sflag, &code);
+    for (int s = r.s0; s <= r.s1; s++) {
+      const int pos = off[s] + base[s] + atomicAdd(&lc[s], 1);
+      if (pos < p.bin_cap) bins[pos] = t | ((r.code == 2) ? (int)0x80000000 : 0);
+    }
+  }
+}
+
+// ---------------------------------------------------------------- K3 strip
+
+constexpr int kChunk = 256;   // triangles staged per pass (== blockDim.x)
+
+struct StripSmem {
+  int* heads;        // [H*G]
+  unsigned* ekey;    // [C]
+  unsigned* et;      // [C]
+  unsigned* elo;     // [C]
+  int* enext;        // [C]
+  uint8_t* emark;    // [C]
+  // triangle chunk
+  float4* q0; float4* q1; float4* q2; float4* q3; float4* q4;   // [kChunk]
+  int4* tm;          // [kChunk] t, x0, y0, ylen
+  int4* tm2;         // [kChunk] xc0, npix, kind, 0
+  int* pref;         // [kChunk + 1]
+  int* thit;         // [kChunk]
+  // per-slot results (aliases the chunk area after rasterization)
+  int* rvo; int* rvss; int* rtc;
+};
+
+struct ColState {
+  int started, ex, im, tc_done;
+  int al, be, ssb, ssa, tc, nvb, nva;
+  int lastz, lasttype, has10, n;
+};
+
+__device__ __forceinline__ void col_init(ColState& s)
+{
+  s.started = s.ex = s.im = s.tc_done = 0;
+  s.al = s.be = s.ssb = s.ssa = s.tc = s.nvb = s.nva = 0;
+  s.lastz = 0; s.lasttype = 0; s.has10 = 0; s.n = 0;
+}
+
+// One pixel of a column, visited in (z desc, nz desc) order: splitAlBe
+// (STomoSh_INT3.cpp:493-513), matchAlBePairBriefly (:583-611),
+// createShadowBriefly (:749-812), createTCPixels (:734-747) and the sums of
+// createVoPixels / createVss_* (:934-1025).  All are left-to-right scans, so
+// one pass gives the same types.  nz*1000.f > 0.01 is nz >= 1 for int16 nz.
+__device__ __forceinline__ int col_step(ColState& s, int z, int nz, float thr, int explicit_ss)
+{
+  int t = (nz >= 1) ? kAl : ((nz <= -1) ? kBe : 0);
+  if (!s.started && t == kAl) s.started = 1;
+  else if (s.started && t == kBe) s.started = 0;
+  else if (t == kAl || t == kBe) t = 0;
+  if (t & kBe) {
+    const float pn = __fdiv_rn((float)nz, 1000.0f);
+    if (pn < 0.001f) {
+      if (!s.ex && pn < thr) { t |= kSSB; s.ex = 1; }
+      if (!s.im && pn > thr) { t |= kNVB; s.im = 1; }
+    }
+  } else if (t & kAl) {
+    if (s.ex) { t |= kSSA; s.ex = 0; }
+    if (s.im) { t |= kNVA; s.im = 0; }
+  }
+  if (!explicit_ss && !s.tc_done && (t & kAl)) { t |= kTC; s.tc_done = 1; }
+  if (t & kAl) {
+    s.al += z;
+    if (t & kTC) s.tc += z;
+    if (t & kNVA) s.nva += z;
+  } else if (t & kBe) {
+    s.be += z;
+    if (t & kNVB) s.nvb += z;
+  }
+  if (t & kSSB) s.ssb += z;
+  else if (t & kSSA) s.ssa += z;
+  s.lastz = z; s.lasttype = t;
+  if (z == 1 && nz == 0) s.has10 = 1;
+  s.n++;
+  return t;
+}
+
+// Close a column of n >= 2 pixels: floor sentinels (STomoSh_INT3.cpp:790-810).
+__device__ __forceinline__ int col_finish(ColState& s)
+{
+  int n = s.n;
+  if (s.ex && n < kSlotCap) { n++; s.lastz = 0; s.lasttype = kSSA; }
+  if (s.im && n < kSlotCap) { n++; s.lastz = 0; s.lasttype = kNVA; }
+  return n;
+}
+
+__device__ __forceinline__ bool prio_less(unsigned ta, unsigned la, unsigned tb, unsigned lb)
+{
+  return (ta < tb) || (ta == tb && la < lb);
+}
+
+struct ColOut { int vo, vss, tc, ndist, nfin, lastz, lasttype, has10; };
+
+__device__ void dump_key(const EngineParams& p, int gslot, int i, unsigned key, int type);
+
+// Column stage of one slot from its shared-memory list.
+__device__ ColOut column(const EngineParams& p, const StripSmem& sm, int head, bool dump, int gslot)
+{
+  ColOut r;
+  r.vo = r.vss = r.tc = 0; r.ndist = 0; r.nfin = 0; r.lastz = 0; r.lasttype = 0; r.has10 = 0;
+  if (head < 0) return r;
+  int n = 0;
+  for (int e = head; e >= 0 && n <= 16; e = sm.enext[e]) n++;
+  ColState s;
+  col_init(s);
+  if (n <= 16) {
+    unsigned k[16];
+    int m = 0;
+#pragma unroll
+    for (int i = 0; i < 16; i++) k[i] = 0u;
+    for (int e = head; e >= 0; e = sm.enext[e]) {
+      const unsigned key = sm.ekey[e];
+      bool dup = false;
+#pragma unroll
+      for (int i = 0; i < 16; i++) dup |= (i < m) && (k[i] == key);
+      if (!dup) {
+        unsigned cur = key;
+#pragma unroll
+        for (int i = 0; i < 16; i++) {
+          if (i < m) { const unsigned a = k[i]; const bool sw = cur > a; k[i] = sw ? cur : a; cur = sw ? a : cur; }
+          else if (i == m) k[i] = cur;
+        }
+        m++;
+      }
+    }
+    r.ndist = m;
+    if (m == 1) {
+      r.nfin = 1; r.lastz = key_z(k[0]); r.lasttype = 0; r.has10 = (key_z(k[0]) == 1 && key_nz(k[0]) == 0);
+      if (dump) dump_key(p, gslot, 0, k[0], 0);
+      return r;
+    }
+#pragma unroll
+    for (int i = 0; i < 16; i++) {
+      if (i < m) {
+        const int t = col_step(s, key_z(k[i]), key_nz(k[i]), p.thr, p.explicit_ss);
+        if (dump) dump_key(p, gslot, i, k[i], t);
+      }
+    }
+  } else {
+    // Long list: first-come dedup and the 63-pixel cap need the priorities.
+    // A pixel is kept iff it is the first (lowest priority) entry of its key
+    // and fewer than 63 such first entries precede it (SetBit semantics).
+    int d = 0;
+    for (int e = head; e >= 0; e = sm.enext[e]) {
+      bool rep = true;
+      for (int f = head; f >= 0; f = sm.enext[f])
+        if (f != e && sm.ekey[f] == sm.ekey[e] && prio_less(sm.et[f], sm.elo[f], sm.et[e], sm.elo[e])) { rep = false; break; }
+      sm.emark[e] = rep ? 1 : 0;
+      d += rep;
+    }
+    if (d > kSlotCap) {
+      for (int e = head; e >= 0; e = sm.enext[e]) {
+        if (!sm.emark[e]) continue;
+        int rank = 0;
+        for (int f = head; f >= 0; f = sm.enext[f])
+          if (sm.emark[f] && prio_less(sm.et[f], sm.elo[f], sm.et[e], sm.elo[e])) rank++;
+        if (rank >= kSlotCap) sm.emark[e] = 2;   // dropped by the cap
+      }
+      d = kSlotCap;
+    }
+    r.ndist = d;
+    if (d == 1) {
+      for (int e = head; e >= 0; e = sm.enext[e])
+        if (sm.emark[e] == 1) {
+          r.nfin = 1; r.lastz = key_z(sm.ekey[e]); r.has10 = (r.lastz == 1 && key_nz(sm.ekey[e]) == 0);
+          if (dump) dump_key(p, gslot, 0, sm.ekey[e], 0);
+          break;
+        }
+      return r;
+    }
+    unsigned long long prev = 0x100000000ull;
+    for (int i = 0; i < d; i++) {
+      int best = -1;
+      for (int e = head; e >= 0; e = sm.enext[e])
+        if (sm.emark[e] == 1 && (unsigned long long)sm.ekey[e] < prev && (best < 0 || sm.ekey[e] > sm.ekey[best])) best = e;
+      if (best < 0) break;
+      const int t = col_step(s, key_z(sm.ekey[best]), key_nz(sm.ekey[best]), p.thr, p.explicit_ss);
+      if (dump) dump_key(p, gslot, i, sm.ekey[best], t);
+      prev = sm.ekey[best];
+    }
+  }
+  r.nfin = col_finish(s);
+  r.vo = (s.al > s.be) ? (s.al - s.be) : 0;
+  r.vss = p.explicit_ss ? (s.ssb - s.ssa) : (-s.al + s.be + s.tc - s.nvb + s.nva);
+  r.tc = s.tc;
+  r.lastz = s.lastz; r.lasttype = s.lasttype; r.has10 = s.has10;
+  return r;
+}
+
+__device__ void dump_key(const EngineParams& p, int gslot, int i, unsigned key, int type)
+{
+  if (p.dump_keys == nullptr || i >= 64) return;
+  p.dump_keys[(size_t)gslot * 64 + i] = key;
+  p.dump_types[(size_t)gslot * 64 + i] = (short)type;
+}
+
+// Bed bookkeeping of one slot (GenerateBed, STomoSh_INT3.cpp:1414-1430).
+__device__ __forceinline__ uint8_t bed_flags(const EngineParams& p, const ColOut& c)
+{
+  if (c.ndist == 0) return kBfPoss | kBfLand;
+  uint8_t f = kBfOcc;
+  const int lt = c.lasttype;
+  const bool floor_type = (lt & kAl) || (lt & kBe) || (lt & kSSA) || (lt & kSS);
+  if (c.lastz == 0 && floor_type) f |= kBfTouch;
+  bool poss = false;
+  if (c.lastz == 0) {
+    if (lt == kNVA || lt == kVo || lt == kVss) poss = true;
+    if (floor_type) poss = false;
+    if (p.bed_type == kBedRaft && ((lt & kBe) || (lt & kSSA))) poss = true;
+  }
+  if (poss) f |= kBfPoss;
+  if (c.nfin < kSlotCap || c.has10) f |= kBfLand;
+  if ((f & kBfTouch) && poss && c.nfin < kSlotCap && !c.has10) f |= kBfSelfR;
+  return f;
+}
+
+__device__ __forceinline__ void emit(const EngineParams& p, const StripSmem& sm, int* nent, int* sflag,
+                                     int xs0, int xs1, int sx, int sy, int z, int nz, unsigned t, unsigned lo)
+{
+  if (sx < 0 || sx >= p.G || sy < 0 || sy >= p.G) { atomicOr(sflag, kFlagGrid); return; }
+  if (sx < xs0 || sx >= xs1) { if (p.mode == 0) atomicOr(sflag, kFlagStray); return; }
+  const int e = atomicAdd(nent, 1);
+  if (e >= p.ent_cap) { atomicOr(sflag, p.mode == 0 ? kFlagOverflow : kFlagSafeOverflow); return; }
+  sm.ekey[e] = make_key(z, nz);
+  sm.et[e] = t;
+  sm.elo[e] = lo;
+  sm.enext[e] = atomicExch(&sm.heads[(sx - xs0) * p.G + sy], e);
+}
+
+__global__ void __launch_bounds__(256, 2) k_strip(EngineParams p)
+{
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ int nent, sflag, wtot[32];
+  __shared__ long long red[8][8];
+
+  const int s = blockIdx.x, o = blockIdx.y;
+  const int HG = p.H * p.G;
+  const int C = p.ent_cap;
+  const int xs0 = s * p.H, xs1 = min(xs0 + p.H, p.G);
+  const int HGs = (xs1 - xs0) * p.G;   // the last strip may be narrower than H
+
+  // shared-memory carve-up (sizes mirrored by strip_smem_bytes on the host)
+  StripSmem sm;
+  unsigned char* q = smem;
+  sm.heads = (int*)q; q += ((sizeof(int) * HG + 15) / 16) * 16;   // keep the float4 arrays 16-byte aligned
+  sm.ekey = (unsigned*)q; q += sizeof(unsigned) * C;
+  sm.et = (unsigned*)q; q += sizeof(unsigned) * C;
+  sm.elo = (unsigned*)q; q += sizeof(unsigned) * C;
+  sm.enext = (int*)q; q += sizeof(int) * C;
+  sm.emark = (uint8_t*)q; q += ((C + 15) / 16) * 16;
+  unsigned char* chunk = q;
+  sm.q0 = (float4*)q; q += sizeof(float4) * kChunk;
+  sm.q1 = (float4*)q; q += sizeof(float4) * kChunk;
+  sm.q2 = (float4*)q; q += sizeof(float4) * kChunk;
+  sm.q3 = (float4*)q; q += sizeof(float4) * kChunk;
+  sm.q4 = (float4*)q; q += sizeof(float4) * kChunk;
+  sm.tm = (int4*)q; q += sizeof(int4) * kChunk;
+  sm.tm2 = (int4*)q; q += sizeof(int4) * kChunk;
+  sm.pref = (int*)q; q += sizeof(int) * (kChunk + 4);
+  sm.thit = (int*)q; q += sizeof(int) * kChunk;
+  sm.rvo = (int*)chunk;
+  sm.rvss = sm.rvo + HG;
+  sm.rtc = sm.rvss + HG;
+
+  for (int i = threadIdx.x; i < HG; i += blockDim.x) sm.heads[i] = -1;
+  if (threadIdx.x == 0) { nent = 0; sflag = 0; }
+  __syncthreads();
+
+  const int* off = p.bin_off + (size_t)o * (p.S + 1);
+  const int lbeg = off[s];
+  const int lend = min(off[s + 1], p.bin_cap);
+  const int nlist = max(lend - lbeg, 0);
+  const int* list = p.bins + (size_t)o * p.bin_cap + lbeg;
+  const Shift sh = load_shift(p, o);
+
+  // ---- phase A: rasterize the strip's triangles into shared memory
+  for (int cb = 0; cb < nlist; cb += kChunk) {
+    const int i = threadIdx.x;
+    int npix = 0;
+    if (cb + i < nlist) {
+      const int entry = list[cb + i];
+      const int t = entry & 0x7FFFFFFF;
+      const int fb_only = (entry < 0) ? 1 : 0;
+      TriGeo g;
+      load_tri(p, o, t, sh, g);
+      Bary b;
+      bary_setup(g, b);
+      int xc0, xc1;
+      if (p.mode == 0) { xc0 = max(g.x0, xs0); xc1 = min(g.x1, xs1 - 1); }
+      else { xc0 = g.x0; xc1 = g.x1; }
+      const int ylen = g.y1 - g.y0 + 1;
+      if (!fb_only && b.ok && xc0 <= xc1 && ylen > 0) npix = (xc1 - xc0 + 1) * ylen;
+      // kind: 1 = fallback only, 2 = box inside this strip (local fallback decision)
+      const int single = (p.mode == 1) || (min(max(g.x0, 0) / p.H, p.S - 1) == min(max(g.x1, 0) / p.H, p.S - 1));
+      sm.q0[i] = make_float4(g.ax, g.ay, g.az, g.n0);
+      sm.q1[i] = make_float4(g.bx, g.by, g.bz, g.n1);
+      sm.q2[i] = make_float4(g.cx, g.cy, g.cz, g.n2);
+      sm.q3[i] = make_float4(b.d00, b.d01, b.d11, b.denom);
+      sm.q4[i] = make_float4(b.e0x, b.e0y, b.e1x, b.e1y);
+      sm.tm[i] = make_int4(t, g.x0, g.y0, ylen);
+      sm.tm2[i] = make_int4(xc0, npix, fb_only | (single << 1), 0);
+    } else {
+      sm.tm2[i] = make_int4(0, 0, 0, 0);
+    }
+    sm.thit[i] = 0;
+    int total;
+    const int start = block_excl_scan(npix, wtot, total);
+    sm.pref[i] = start;
+    if (i == 0) sm.pref[kChunk] = total;
+    __syncthreads();
+    const int nchunk = min(kChunk, nlist - cb);
+    for (int j = threadIdx.x; j < total; j += blockDim.x) {
+      // triangle of work item j: last i with pref[i] <= j
+      int lo = 0, hi = nchunk - 1;
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (sm.pref[mid] <= j) lo = mid; else hi = mid - 1;
+      }
+      const int ti = lo;
+      const int4 tm = sm.tm[ti];
+      const int4 tm2 = sm.tm2[ti];
+      const int k = j - sm.pref[ti];
+      const int x = tm2.x + k / tm.w;
+      const int y = tm.z + k % tm.w;
+      const float4 a4 = sm.q0[ti], b4 = sm.q1[ti], c4 = sm.q2[ti], d4 = sm.q3[ti], e4 = sm.q4[ti];
+      Bary b;
+      b.e0x = e4.x; b.e0y = e4.y; b.e1x = e4.z; b.e1y = e4.w;
+      b.d00 = d4.x; b.d01 = d4.y; b.d11 = d4.z; b.denom = d4.w; b.ok = true;
+      float u, v, w;
+      if (!bary_test(a4.x, a4.y, b, pix_center(x, p.half), pix_center(y, p.half), p.vmax, u, v, w)) continue;
+      sm.thit[ti] = 1;
+      const float px = bary3(a4.x, b4.x, c4.x, u, v, w);
+      const float py = bary3(a4.y, b4.y, c4.y, u, v, w);
+      const float pz = bary3(a4.z, b4.z, c4.z, u, v, w);
+      const float nzf = bary3(a4.w, b4.w, c4.w, u, v, w);
+      const int sx = __float2int_rz(px), sy = __float2int_rz(py);
+      const unsigned lidx = (unsigned)((x - tm.y) * tm.w + (y - tm.z));
+      emit(p, sm, &nent, &sflag, xs0, xs1, sx, sy, to_i16(pz), to_i16(__fmul_rn(nzf, 1000.0f)),
+           (unsigned)tm.x, lidx * 2u);
+      if (p.twin) {
+        const float pz2 = __fadd_rn(pz, (nzf >= 0.0f) ? -p.shell_off : p.shell_off);
+        emit(p, sm, &nent, &sflag, xs0, xs1, sx, sy, to_i16(pz2), to_i16(__fmul_rn(-nzf, 1000.0f)),
+             (unsigned)tm.x, lidx * 2u + 1u);
+      }
+    }
+    __syncthreads();
+    // centroid fallback of triangles without any accepted pixel
+    if (i < nchunk) {
+      const int kind = sm.tm2[i].z;
+      const bool fb = (kind & 1) || ((kind & 2) && sm.thit[i] == 0);
+      if (fb) {
+        const int t = sm.tm[i].x;
+        const int4 ix = p.tri[t];
+        const float4* X = p.xf + (size_t)o * p.nV;
+        const float4 A = X[ix.x], B = X[ix.y], Cc = X[ix.z];
+        const float fx = centroid(__fsub_rn(A.x, sh.dx), __fsub_rn(B.x, sh.dx), __fsub_rn(Cc.x, sh.dx));
+        const float fy = centroid(__fsub_rn(A.y, sh.dy), __fsub_rn(B.y, sh.dy), __fsub_rn(Cc.y, sh.dy));
+        const float fz = centroid(__fsub_rn(A.z, sh.dz), __fsub_rn(B.z, sh.dz), __fsub_rn(Cc.z, sh.dz));
+        const int sx = __float2int_rz(fx), sy = __float2int_rz(fy);
+        emit(p, sm, &nent, &sflag, xs0, xs1, sx, sy, to_i16(fz), to_i16(__fmul_rn(A.w, 1000.0f)), (unsigned)t, 0u);
+        if (p.twin) {
+          const float fz2 = __fadd_rn(fz, (A.w >= 0.0f) ? -p.shell_off : p.shell_off);
+          emit(p, sm, &nent, &sflag, xs0, xs1, sx, sy, to_i16(fz2), to_i16(__fmul_rn(-A.w, 1000.0f)), (unsigned)t, 1u);
+        }
+      }
+    }
+    __syncthreads();
+  }
+
+  const bool redo = (p.mode == 0) && (sflag & (kFlagStray | kFlagOverflow));
+
+  // ---- phase B: column stage, contiguous slot range per thread (keeps slot order)
+  const int per = (HGs + blockDim.x - 1) / blockDim.x;
+  const int sb = min(threadIdx.x * per, HGs);
+  const int se = min(sb + per, HGs);
+  long long a_vo = 0, a_vss = 0, a_tc = 0, a_avss = 0, a_atc = 0, a_ent = 0, a_col = 0;
+  int nkeep = 0;
+  int bx0 = INT_MAX, by0 = INT_MAX, bx1 = -1, by1 = -1;
+  uint8_t* bedf = p.bedf + (size_t)o * p.G * p.G;
+  const bool dump = (o == p.dump_slot) && p.dump_cols != nullptr;
+  if (!redo) {
+    for (int ls = sb; ls < se; ls++) {
+      const int gx = xs0 + ls / p.G, gy = ls % p.G;
+      const int gslot = gx * p.G + gy;
+      const ColOut c = column(p, sm, sm.heads[ls], dump, gslot);
+      sm.rvo[ls] = c.vo; sm.rvss[ls] = c.vss; sm.rtc[ls] = c.tc;
+      if (c.ndist > 1 && (c.vo | c.vss | c.tc)) nkeep++;
+      a_vo += c.vo; a_vss += c.vss; a_tc += c.tc;
+      a_avss += (c.vss < 0) ? -c.vss : c.vss; a_atc += (c.tc < 0) ? -c.tc : c.tc;
+      a_ent += c.ndist;
+      if (c.ndist > 0) {
+        a_col++;
+        bx0 = min(bx0, gx); bx1 = max(bx1, gx); by0 = min(by0, gy); by1 = max(by1, gy);
+      }
+      if (p.bed_type != kBedNone) bedf[gslot] = bed_flags(p, c);
+      if (dump) {
+        int* d = p.dump_cols + (size_t)gslot * 8;
+        d[0] = c.ndist; d[1] = c.nfin; d[2] = c.vo; d[3] = c.vss; d[4] = c.tc; d[5] = c.lastz;
+        d[6] = c.lasttype; d[7] = (p.bed_type != kBedNone) ? bed_flags(p, c) : 0;
+      }
+    }
+  }
+
+  // ---- phase C: reductions and the slot-ordered fold list
+  int ktot;
+  const int kofs = block_excl_scan(nkeep, wtot, ktot);
+  if (!redo) {
+    int4* fv = p.foldv + (size_t)o * p.G * p.G + (size_t)xs0 * p.G;
+    int w = kofs;
+    for (int ls = sb; ls < se; ls++) {
+      const int vo = sm.rvo[ls], vss = sm.rvss[ls], tc = sm.rtc[ls];
+      if ((vo | vss | tc) != 0) fv[w++] = make_int4(vo, vss, tc, ls);
+    }
+  }
+  long long vals[8] = {a_vo, a_vss, a_tc, a_avss, a_atc, a_ent, a_col, (long long)nkeep};
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < 8; k++) {
+    const long long v = warp_sum(vals[k]);
+    if (lane == 0) red[k][wid] = v;
+  }
+  for (int off2 = 16; off2 > 0; off2 >>= 1) {
+    bx0 = min(bx0, __shfl_xor_sync(0xFFFFFFFFu, bx0, off2));
+    by0 = min(by0, __shfl_xor_sync(0xFFFFFFFFu, by0, off2));
+    bx1 = max(bx1, __shfl_xor_sync(0xFFFFFFFFu, bx1, off2));
+    by1 = max(by1, __shfl_xor_sync(0xFFFFFFFFu, by1, off2));
+  }
+  if (lane == 0 && bx1 >= 0 && !redo) {
+    atomicMin(&p.bbox[o * 4 + 0], bx0); atomicMin(&p.bbox[o * 4 + 1], by0);
+    atomicMax(&p.bbox[o * 4 + 2], bx1); atomicMax(&p.bbox[o * 4 + 3], by1);
+  }
+  __syncthreads();
+  if (threadIdx.x < 8) {
+    long long v = 0;
+    for (int w2 = 0; w2 < (int)(blockDim.x >> 5); w2++) v += red[threadIdx.x][w2];
+    if (!redo && v != 0) atomicAdd((unsigned long long*)&p.acc[(size_t)o * kAccLanes + threadIdx.x], (unsigned long long)v);
+  }
+  if (threadIdx.x == 0) {
+    if (!redo) p.foldcnt[(size_t)o * p.S + s] = ktot;
+    if (sflag) atomicOr(&p.flags[o], sflag);
+  }
+}
+
+// ---------------------------------------------------------------- K4 bed
+
+// IsBedCandidate (STomoSh_INT3.cpp:1331-1373) on the slot flags, with the
+// reference's scan order folded in: a raft pixel appended under a floor
+// contact at an earlier scan position hides that contact (kBfSelfR).
+__device__ bool bed_candidate(const EngineParams& p, const uint8_t* bedf, int X, int Y)
+{
+  const int r = p.bed_r;
+  const int xa = max(X - r, 0), xb = min(X + r, p.G);
+  const int ya = max(Y - r, 0), yb = min(Y + r, p.G);
+  const int qid = X * p.G + Y;
+  float md = 1e5f;
+  for (int sx = xa; sx < xb; sx++)
+    for (int sy = ya; sy < yb; sy++) {
+      const int sid = sx * p.G + sy;
+      const uint8_t f = bedf[sid];
+      if (!(f & kBfTouch)) continue;
+      if ((f & kBfSelfR) && sid < qid) continue;
+      const float dxf = __fsub_rn((float)X, (float)sx), dyf = __fsub_rn((float)Y, (float)sy);
+      const float dist = __fsqrt_rn(__fadd_rn(__fmul_rn(dxf, dxf), __fmul_rn(dyf, dyf)));
+      md = (md < dist) ? md : dist;
+    }
+  if (md > p.bed_outer) return false;
+  if (p.bed_type == kBedBrim || p.bed_type == kBedRaft) return true;
+  if (p.bed_type == kBedSkirt && md > p.bed_inner) return true;
+  return false;
+}
+
+__global__ void __launch_bounds__(256) k_bed(EngineParams p)
+{
+  __shared__ int wsum[8];
+  const int o = blockIdx.y;
+  const int fl = p.flags[o];
+  if (fl & (kFlagStray | kFlagOverflow | kFlagBinCap)) return;
+  const int id = p.ori[o];
+  if (p.bed_type == kBedNone || p.bed_r <= 0 || p.bbox[o * 4 + 2] < 0) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) p.out_nbed[id] = 0;
+    return;
+  }
+  const int m = (int)p.bed_outer + 1;
+  const int bx0 = max(p.bbox[o * 4 + 0] - m, 0), bx1 = min(p.bbox[o * 4 + 2] + m + 1, p.G);
+  const int by0 = max(p.bbox[o * 4 + 1] - m, 0), by1 = min(p.bbox[o * 4 + 3] + m + 1, p.G);
+  const int w = by1 - by0;
+  const int n = (bx1 - bx0) * w;
+  const uint8_t* bedf = p.bedf + (size_t)o * p.G * p.G;
+  int cnt = 0;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+    const int X = bx0 + q / w, Y = by0 + q % w;
+    const uint8_t f = bedf[X * p.G + Y];
+    if ((f & kBfPoss) && (f & kBfLand) && bed_candidate(p, bedf, X, Y)) cnt++;
+  }
+  cnt = warp_sum(cnt);
+  if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = cnt;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int t = 0;
+    for (int k = 0; k < 8; k++) t += wsum[k];
+    if (t) atomicAdd(&p.out_nbed[id], t);
+  }
+}
+
+// ---------------------------------------------------------------- K5 fold / outputs
+// Per orientation: the reference accumulates Vo, Vss (Pairing,
+// STomoSh_INT3.cpp:375-392) and Vtc (Calculate, :1237) in float32 over
+// columns in ascending slot order.  While every partial sum stays within
+// 2^24 in magnitude that fold is exact and equals the int64 total; otherwise
+// it is replayed sequentially from the slot-ordered column values, one
+// orientation per lane.
+
+__global__ void __launch_bounds__(64) k_fold(EngineParams p)
+{
+  const int o = blockIdx.x * blockDim.x + threadIdx.x;
+  if (o >= p.Bo) return;
+  const int id = p.ori[o];
+  const int fl = p.flags[o];
+  p.out_flags[id] = fl;
+  if (fl & (kFlagStray | kFlagOverflow | kFlagBinCap)) return;
+  const long long* a = p.acc + (size_t)o * kAccLanes;
+  const long long vo = a[kAccVo], vss = a[kAccVss], vtc = a[kAccVtc];
+  p.out_vo[id] = vo; p.out_vss[id] = vss; p.out_vtc[id] = vtc;
+  p.out_entries[id] = a[kAccEntries]; p.out_columns[id] = a[kAccColumns];
+  const long long lim = 1ll << 24;
+  if (vo <= lim && a[kAccAbsVss] <= lim && a[kAccAbsVtc] <= lim) {
+    p.out_vof[id] = (float)vo; p.out_vssf[id] = (float)vss; p.out_vtcf[id] = (float)vtc;
+    return;
+  }
+  float fo = 0.f, fs = 0.f, ft = 0.f;
+  const int4* fv = p.foldv + (size_t)o * p.G * p.G;
+  const int* fc = p.foldcnt + (size_t)o * p.S;
+  for (int s = 0; s < p.S; s++) {
+    const int n = fc[s];
+    const int4* v = fv + (size_t)s * p.H * p.G;
+    for (int k = 0; k < n; k++) {
+      const int4 x = v[k];
+      fo = __fadd_rn(fo, (float)x.x);
+      fs = __fadd_rn(fs, (float)x.y);
+      ft = __fadd_rn(ft, (float)x.z);
+    }
+  }
+  p.out_vof[id] = fo; p.out_vssf[id] = fs; p.out_vtcf[id] = ft;
+}
+
+}  // namespace tomo
+
+// ---------------------------------------------------------------- launchers
+
+namespace tomo {
+
+size_t strip_smem_bytes(int H, int G, int ent_cap)
+{
+  const size_t HG = (size_t)H * G;
+  size_t b = ((sizeof(int) * HG + 15) / 16) * 16;      // heads, padded to 16 bytes
+  b += 4 * sizeof(unsigned) * (size_t)ent_cap;          // key, t, lo, next
+  b += (((size_t)ent_cap + 15) / 16) * 16;              // marks
+  const size_t chunk = 5 * sizeof(float4) * kChunk + 2 * sizeof(int4) * kChunk + sizeof(int) * (2 * kChunk + 4);
+  const size_t results = 3 * sizeof(int) * HG;
+  b += (chunk > results) ? chunk : results;
+  return b;
+}
+
+cudaError_t configure_kernels(size_t strip_smem)
+{
+  cudaError_t e = cudaFuncSetAttribute(k_strip, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)strip_smem);
+  if (e != cudaSuccess) return e;
+  return cudaSuccess;
+}
+
+// Everything of one batch except the fold; the fold goes to `side` after
+// `ready` is recorded on `main`.
+cudaError_t launch_batch(const EngineParams& p, cudaStream_t main, size_t strip_smem)
+{
+  k_reset<<<p.Bo, 256, 0, main>>>(p);
+  const int rot_blocks = (p.nV + 255) / 256 < 64 ? (p.nV + 255) / 256 : 64;
+  k_rotate<<<dim3(rot_blocks > 0 ? rot_blocks : 1, p.Bo), 256, 0, main>>>(p);
+  const int tri_blocks = (p.nT + 255) / 256 < 64 ? (p.nT + 255) / 256 : 64;
+  const dim3 tg(tri_blocks > 0 ? tri_blocks : 1, p.Bo);
+  k_bin_count<<<tg, 256, sizeof(int) * p.S, main>>>(p);
+  k_bin_scan<<<p.Bo, 1024, 0, main>>>(p);
+  k_bin_fill<<<tg, 256, 2 * sizeof(int) * p.S, main>>>(p);
+  k_strip<<<dim3(p.S, p.Bo), 256, strip_smem, main>>>(p);
+  k_bed<<<dim3(8, p.Bo), 256, 0, main>>>(p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fold(const EngineParams& p, cudaStream_t side)
+{
+  k_fold<<<(p.Bo + 63) / 64, 64, 0, side>>>(p);
+  return cudaGetLastError();
+}
+
+// Count pass only (safe mode sizes its bin buffer from the exact totals).
+cudaError_t launch_bin_count(const EngineParams& p, cudaStream_t main)
+{
+  k_reset<<<p.Bo, 256, 0, main>>>(p);
+  const int rot_blocks = (p.nV + 255) / 256 < 64 ? (p.nV + 255) / 256 : 64;
+  k_rotate<<<dim3(rot_blocks > 0 ? rot_blocks : 1, p.Bo), 256, 0, main>>>(p);
+  const int tri_blocks = (p.nT + 255) / 256 < 64 ? (p.nT + 255) / 256 : 64;
+  const dim3 tg(tri_blocks > 0 ? tri_blocks : 1, p.Bo);
+  k_bin_count<<<tg, 256, sizeof(int) * p.S, main>>>(p);
+  k_bin_scan<<<p.Bo, 1024, 0, main>>>(p);
+  return cudaGetLastError();
+}
+
+// Remainder of a batch after launch_bin_count.
+cudaError_t launch_after_count(const EngineParams& p, cudaStream_t main, size_t strip_smem)
+{
+  const int tri_blocks = (p.nT + 255) / 256 < 64 ? (p.nT + 255) / 256 : 64;
+  const dim3 tg(tri_blocks > 0 ? tri_blocks : 1, p.Bo);
+  k_bin_fill<<<tg, 256, 2 * sizeof(int) * p.S, main>>>(p);
+  k_strip<<<dim3(p.S, p.Bo), 256, strip_smem, main>>>(p);
+  k_bed<<<dim3(8, p.Bo), 256, 0, main>>>(p);
+  return cudaGetLastError();
+}
+
+}  // namespace tomo
