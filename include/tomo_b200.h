@@ -102,6 +102,15 @@ int tomoPrepare(const float* f32info, const int* i32info, const float* YPR, cons
 int tomoSweepDevice(void* ev_start, void* ev_stop, float* kernel_ms);
 int tomoFinish(float* Mo, float* Mss, float* Vtc);
 
+/* Launch accounting.  Kernel kinds, in order: reset, rotate, bin_count,
+ * bin_scan, bin_fill, strip, bed, fold.  tomoProfile(enable, reset) turns
+ * per-launch CUDA-event timing on or off (events are recorded on the stream
+ * each kernel is launched on) and optionally clears the log;
+ * tomoGetKernelLog fills launches / total ms / timed launches per kind and
+ * returns the number of kinds. */
+int tomoProfile(int enable, int reset);
+int tomoGetKernelLog(long long* launches, double* ms, long long* timed, int n);
+
 /* Slot grid edge G of the prepared mesh (slot id = x * G + y). */
 int tomoGridSize(void);
 

@@ -9,6 +9,7 @@
 
 #include <cstdint>
 #include <cuda_runtime.h>
+#include <vector>
 
 namespace tomo {
 
@@ -98,6 +99,7 @@ struct EngineParams {
   uint8_t* bedf;        // [Bo][G*G]
   int* foldcnt;         // [Bo][S]
   int4* foldv;          // [Bo][G*G] (vo, vss, tc, local slot)
+  int* foldmeta;        // [Bo][S][8] per strip: sum vo, vss, tc, |vss|, |tc|
 
   // per-orientation outputs (indexed by orientation id)
   long long* out_vo;
@@ -116,6 +118,55 @@ struct EngineParams {
   int* dump_cols;       // [G*G][8]: n_distinct, n_final, vo, vss, tc, last_z, last_type, flags
   unsigned* dump_keys;  // [G*G][64] kept (z, nz) keys in column order, or null
   short* dump_types;    // [G*G][64] their final types
+};
+
+// Kernel kinds for launch accounting.
+enum : int { kKReset = 0, kKRotate, kKCount, kKScan, kKFill, kKStrip, kKBed, kKFold, kKinds };
+
+// Host-side launch log: launch counts per kernel kind and, when timing is
+// on, one event pair per launch recorded on the launching stream.
+struct LaunchLog {
+  struct Span { int kind; cudaEvent_t start, stop; };
+  bool timing = false;
+  long long launches[kKinds] = {0};
+  double ms[kKinds] = {0};
+  long long timed[kKinds] = {0};
+  std::vector<Span> pending;
+  std::vector<cudaEvent_t> pool;
+  size_t next = 0;
+
+  cudaEvent_t take_event()
+  {
+    if (next == pool.size()) {
+      cudaEvent_t e = nullptr;
+      cudaEventCreate(&e);
+      pool.push_back(e);
+    }
+    return pool[next++];
+  }
+  // Fold the pending spans into ms[] (the streams must be idle).
+  void collect()
+  {
+    for (const Span& s : pending) {
+      float t = 0.f;
+      if (cudaEventElapsedTime(&t, s.start, s.stop) == cudaSuccess) { ms[s.kind] += t; timed[s.kind]++; }
+    }
+    pending.clear();
+    next = 0;
+  }
+  void reset()
+  {
+    pending.clear();
+    next = 0;
+    for (int k = 0; k < kKinds; k++) { launches[k] = 0; ms[k] = 0; timed[k] = 0; }
+  }
+  void destroy()
+  {
+    for (cudaEvent_t e : pool) cudaEventDestroy(e);
+    pool.clear();
+    pending.clear();
+    next = 0;
+  }
 };
 
 }  // namespace tomo

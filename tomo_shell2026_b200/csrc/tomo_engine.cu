@@ -28,10 +28,10 @@ namespace tomo {
 
 size_t strip_smem_bytes(int H, int G, int ent_cap);
 cudaError_t configure_kernels(size_t strip_smem);
-cudaError_t launch_batch(const EngineParams& p, cudaStream_t main, size_t strip_smem);
-cudaError_t launch_fold(const EngineParams& p, cudaStream_t side);
-cudaError_t launch_bin_count(const EngineParams& p, cudaStream_t main);
-cudaError_t launch_after_count(const EngineParams& p, cudaStream_t main, size_t strip_smem);
+cudaError_t launch_batch(const EngineParams& p, cudaStream_t main, size_t strip_smem, LaunchLog* L);
+cudaError_t launch_fold(const EngineParams& p, cudaStream_t side, LaunchLog* L);
+cudaError_t launch_bin_count(const EngineParams& p, cudaStream_t main, LaunchLog* L);
+cudaError_t launch_after_count(const EngineParams& p, cudaStream_t main, size_t strip_smem, LaunchLog* L);
 
 namespace {
 
@@ -176,6 +176,7 @@ struct BatchSet {   // per-batch buffers read by the fold, double-buffered
   DevBuf<int> flags;
   DevBuf<int> foldcnt;
   DevBuf<int4> foldv;
+  DevBuf<int> foldmeta;
   cudaEvent_t folded = nullptr;
 };
 
@@ -225,6 +226,8 @@ struct Engine {
   float mat4x4[16] = {0};
   double last_kernel_ms = 0.0;
   int n_safe = 0;
+  int H_sweep = 0;        // strip height of the last normal sweep
+  LaunchLog log;
 
   int init()
   {
@@ -247,10 +250,11 @@ struct Engine {
     vpos.release(); vnrm.release(); tri.release(); rot.release(); ori.release();
     xf.release(); minkey.release(); tcode.release(); bin_off.release(); bin_cur.release(); bins.release();
     bbox.release(); bedf.release();
-    for (auto& s : set) { s.acc.release(); s.flags.release(); s.foldcnt.release(); s.foldv.release(); }
+    for (auto& s : set) { s.acc.release(); s.flags.release(); s.foldcnt.release(); s.foldv.release(); s.foldmeta.release(); }
     o_vo.release(); o_vss.release(); o_vtc.release(); o_ent.release(); o_col.release();
     o_vof.release(); o_vssf.release(); o_vtcf.release(); o_nbed.release(); o_flags.release();
     dump_cols.release(); dump_keys.release(); dump_types.release();
+    log.destroy();
     if (main) { cudaStreamDestroy(main); main = nullptr; }
     if (side) { cudaStreamDestroy(side); side = nullptr; }
     if (ev_ready) { cudaEventDestroy(ev_ready); ev_ready = nullptr; }
@@ -392,6 +396,7 @@ struct Engine {
       TOMO_CUDA(s.flags.reserve((size_t)Bo));
       TOMO_CUDA(s.foldcnt.reserve((size_t)Bo * S));
       TOMO_CUDA(s.foldv.reserve((size_t)Bo * GG));
+      TOMO_CUDA(s.foldmeta.reserve((size_t)Bo * S * 8));
     }
     return 0;
   }
@@ -414,7 +419,7 @@ struct Engine {
     p.bin_off = bin_off.ptr; p.bin_cur = bin_cur.ptr; p.bins = bins.ptr; p.bin_cap = bin_cap;
     p.bbox = bbox.ptr; p.bedf = bedf.ptr;
     p.acc = set[which].acc.ptr; p.flags = set[which].flags.ptr;
-    p.foldcnt = set[which].foldcnt.ptr; p.foldv = set[which].foldv.ptr;
+    p.foldcnt = set[which].foldcnt.ptr; p.foldv = set[which].foldv.ptr; p.foldmeta = set[which].foldmeta.ptr;
   }
 
   // All orientations in normal mode (or safe mode when forced), asynchronously on `main`.
@@ -423,6 +428,7 @@ struct Engine {
     if (nYPR == 0 || P.n_tri == 0) return 0;
     const int mode = force_safe ? 1 : 0;
     choose_strips(mode);
+    H_sweep = H;
     const size_t smem = strip_smem_bytes(H, G, ent_cap);
     TOMO_CUDA(configure_kernels(smem));
     const int Bo = std::min(batch, nYPR);
@@ -438,10 +444,10 @@ struct Engine {
       const int which = k & 1;
       if (k >= 2) TOMO_CUDA(cudaStreamWaitEvent(main, set[which].folded, 0));
       bind_batch(p, nb, bin_cap, which, first);
-      TOMO_CUDA(launch_batch(p, main, smem));
+      TOMO_CUDA(launch_batch(p, main, smem, &log));
       TOMO_CUDA(cudaEventRecord(ev_ready, main));
       TOMO_CUDA(cudaStreamWaitEvent(side, ev_ready, 0));
-      TOMO_CUDA(launch_fold(p, side));
+      TOMO_CUDA(launch_fold(p, side, &log));
       TOMO_CUDA(cudaEventRecord(set[which].folded, side));
     }
     // join the side stream back into main
@@ -470,7 +476,7 @@ struct Engine {
       // The count pass decides the bin capacity, so it runs without one.
       bind_batch(p, nb, INT_MAX, 0, 0);
       p.ori = sub.ptr + first;
-      TOMO_CUDA(launch_bin_count(p, main));
+      TOMO_CUDA(launch_bin_count(p, main, &log));
       std::vector<int> off((size_t)nb * (S + 1));
       TOMO_CUDA(cudaMemcpyAsync(off.data(), bin_off.ptr, sizeof(int) * off.size(), cudaMemcpyDeviceToHost, main));
       TOMO_CUDA(cudaStreamSynchronize(main));
@@ -479,8 +485,8 @@ struct Engine {
       TOMO_CUDA(bins.reserve((size_t)nb * cap));
       p.bins = bins.ptr; p.bin_cap = cap;
       for (int o = 0; o < nb; o++) TOMO_CUDA(cudaMemsetAsync(o_nbed.ptr + ids[first + o], 0, sizeof(int), main));
-      TOMO_CUDA(launch_after_count(p, main, smem));
-      TOMO_CUDA(launch_fold(p, main));
+      TOMO_CUDA(launch_after_count(p, main, smem, &log));
+      TOMO_CUDA(launch_fold(p, main, &log));
       TOMO_CUDA(cudaStreamSynchronize(main));
     }
     sub.release();
@@ -514,6 +520,8 @@ struct Engine {
     TOMO_CUDA(cudaMemcpyAsync(nbed.data(), o_nbed.ptr, sizeof(int) * n, cudaMemcpyDeviceToHost, main));
     TOMO_CUDA(cudaMemcpyAsync(flags.data(), o_flags.ptr, sizeof(int) * n, cudaMemcpyDeviceToHost, main));
     TOMO_CUDA(cudaStreamSynchronize(main));
+    TOMO_CUDA(cudaStreamSynchronize(side));
+    log.collect();
     return 0;
   }
 
@@ -566,18 +574,18 @@ struct Engine {
     TOMO_TRY(reserve_batch(1, mode == 0 ? cap : 1));
     bind_batch(p, 1, mode == 0 ? cap : INT_MAX, 0, id);
     if (mode == 0) {
-      TOMO_CUDA(launch_batch(p, main, smem));
+      TOMO_CUDA(launch_batch(p, main, smem, &log));
     } else {
-      TOMO_CUDA(launch_bin_count(p, main));
+      TOMO_CUDA(launch_bin_count(p, main, &log));
       int total = 0;
       TOMO_CUDA(cudaMemcpyAsync(&total, bin_off.ptr + S, sizeof(int), cudaMemcpyDeviceToHost, main));
       TOMO_CUDA(cudaStreamSynchronize(main));
       cap = std::max(total, 1);
       TOMO_CUDA(bins.reserve((size_t)cap));
       p.bins = bins.ptr; p.bin_cap = cap;
-      TOMO_CUDA(launch_after_count(p, main, smem));
+      TOMO_CUDA(launch_after_count(p, main, smem, &log));
     }
-    TOMO_CUDA(launch_fold(p, main));
+    TOMO_CUDA(launch_fold(p, main, &log));
     if (cols8) TOMO_CUDA(cudaMemcpyAsync(cols8, dump_cols.ptr, sizeof(int) * GG * 8, cudaMemcpyDeviceToHost, main));
     if (keys64) TOMO_CUDA(cudaMemcpyAsync(keys64, dump_keys.ptr, sizeof(unsigned) * GG * 64, cudaMemcpyDeviceToHost, main));
     if (types64) TOMO_CUDA(cudaMemcpyAsync(types64, dump_types.ptr, sizeof(short) * GG * 64, cudaMemcpyDeviceToHost, main));
@@ -747,7 +755,8 @@ int tomoGetStats(long long* out, int n)
   std::lock_guard<std::mutex> lock(g_mutex);
   if (!g_engine || out == nullptr) return TOMO_ERR_ARG;
   const Engine& E = *g_engine;
-  const long long v[8] = {E.G, E.H, E.S, E.ent_cap, E.n_safe, E.nYPR, E.batch, 0};
+  const long long v[8] = {E.G, E.H_sweep, (E.G + std::max(E.H_sweep, 1) - 1) / std::max(E.H_sweep, 1),
+                          E.ent_cap, E.n_safe, E.nYPR, E.batch, 0};
   for (int i = 0; i < n && i < 8; i++) out[i] = v[i];
   return 0;
 }
@@ -810,6 +819,28 @@ int tomoSweepDevice(void* ev_start, void* ev_stop, float* kernel_ms)
   if (la) cudaEventDestroy(la);
   if (lb) cudaEventDestroy(lb);
   return rc;
+}
+
+int tomoProfile(int enable, int reset)
+{
+  std::lock_guard<std::mutex> lock(g_mutex);
+  Engine& E = engine();
+  if (reset) E.log.reset();
+  E.log.timing = enable != 0;
+  return 0;
+}
+
+int tomoGetKernelLog(long long* launches, double* ms, long long* timed, int n)
+{
+  std::lock_guard<std::mutex> lock(g_mutex);
+  if (!g_engine) return TOMO_ERR_ARG;
+  const LaunchLog& L = g_engine->log;
+  for (int k = 0; k < n && k < kKinds; k++) {
+    if (launches) launches[k] = L.launches[k];
+    if (ms) ms[k] = L.ms[k];
+    if (timed) timed[k] = L.timed[k];
+  }
+  return kKinds;
 }
 
 int tomoGridSize(void)

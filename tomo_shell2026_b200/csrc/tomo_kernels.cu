@@ -833,6 +833,8 @@ __global__ void __launch_bounds__(256, 2) k_strip(EngineParams p)
     long long v = 0;
     for (int w2 = 0; w2 < (int)(blockDim.x >> 5); w2++) v += red[threadIdx.x][w2];
     if (!redo && v != 0) atomicAdd((unsigned long long*)&p.acc[(size_t)o * kAccLanes + threadIdx.x], (unsigned long long)v);
+    // strip sums for the fold: |column value| <= 2 * grid, so a strip sum fits in int32
+    if (!redo && threadIdx.x < 5) p.foldmeta[((size_t)o * p.S + s) * 8 + threadIdx.x] = (int)v;
   }
   if (threadIdx.x == 0) {
     if (!redo) p.foldcnt[(size_t)o * p.S + s] = ktot;
@@ -904,42 +906,75 @@ __global__ void __launch_bounds__(256) k_bed(EngineParams p)
 // ---------------------------------------------------------------- K5 fold / outputs
 // Per orientation: the reference accumulates Vo, Vss (Pairing,
 // STomoSh_INT3.cpp:375-392) and Vtc (Calculate, :1237) in float32 over
-// columns in ascending slot order.  While every partial sum stays within
-// 2^24 in magnitude that fold is exact and equals the int64 total; otherwise
-// it is replayed sequentially from the slot-ordered column values, one
-// orientation per lane.
+// columns in ascending slot order.  A float32 fold of integers is exact while
+// every partial sum stays within 2^24 in magnitude.  The per-strip exact sums
+// and absolute sums written by k_strip bound every partial sum inside a
+// strip, so whole strips are skipped exactly until the first strip where the
+// bound could pass 2^24; from there the fold is replayed value by value in
+// slot order (staged through shared memory, folded by one thread).  One CTA
+// per orientation.
 
-__global__ void __launch_bounds__(64) k_fold(EngineParams p)
+constexpr int kFoldChunk = 1024;
+
+__global__ void __launch_bounds__(128) k_fold(EngineParams p)
 {
-  const int o = blockIdx.x * blockDim.x + threadIdx.x;
+  __shared__ int4 stage[kFoldChunk];
+  __shared__ int s_start;
+  __shared__ long long s_pre[3];
+  __shared__ float s_f[3];
+  const int o = blockIdx.x;
   if (o >= p.Bo) return;
   const int id = p.ori[o];
   const int fl = p.flags[o];
-  p.out_flags[id] = fl;
+  if (threadIdx.x == 0) p.out_flags[id] = fl;
   if (fl & (kFlagStray | kFlagOverflow | kFlagBinCap)) return;
   const long long* a = p.acc + (size_t)o * kAccLanes;
-  const long long vo = a[kAccVo], vss = a[kAccVss], vtc = a[kAccVtc];
-  p.out_vo[id] = vo; p.out_vss[id] = vss; p.out_vtc[id] = vtc;
-  p.out_entries[id] = a[kAccEntries]; p.out_columns[id] = a[kAccColumns];
+  const int* meta = p.foldmeta + (size_t)o * p.S * 8;
   const long long lim = 1ll << 24;
-  if (vo <= lim && a[kAccAbsVss] <= lim && a[kAccAbsVtc] <= lim) {
-    p.out_vof[id] = (float)vo; p.out_vssf[id] = (float)vss; p.out_vtcf[id] = (float)vtc;
-    return;
+  if (threadIdx.x == 0) {
+    p.out_vo[id] = a[kAccVo]; p.out_vss[id] = a[kAccVss]; p.out_vtc[id] = a[kAccVtc];
+    p.out_entries[id] = a[kAccEntries]; p.out_columns[id] = a[kAccColumns];
+    // first strip where some channel's partial sums could leave [-2^24, 2^24]
+    long long pre[3] = {0, 0, 0};
+    int start = p.S;
+    for (int s = 0; s < p.S; s++) {
+      const long long sv[3] = {meta[s * 8 + 0], meta[s * 8 + 1], meta[s * 8 + 2]};
+      const long long ab[3] = {meta[s * 8 + 0], meta[s * 8 + 3], meta[s * 8 + 4]};   // vo >= 0
+      bool cross = false;
+      for (int c = 0; c < 3; c++) {
+        const long long m = (pre[c] < 0 ? -pre[c] : pre[c]) + ab[c];
+        if (m > lim) cross = true;
+      }
+      if (cross) { start = s; break; }
+      for (int c = 0; c < 3; c++) pre[c] += sv[c];
+    }
+    s_start = start;
+    for (int c = 0; c < 3; c++) { s_pre[c] = pre[c]; s_f[c] = (float)pre[c]; }
   }
-  float fo = 0.f, fs = 0.f, ft = 0.f;
-  const int4* fv = p.foldv + (size_t)o * p.G * p.G;
-  const int* fc = p.foldcnt + (size_t)o * p.S;
-  for (int s = 0; s < p.S; s++) {
-    const int n = fc[s];
-    const int4* v = fv + (size_t)s * p.H * p.G;
-    for (int k = 0; k < n; k++) {
-      const int4 x = v[k];
-      fo = __fadd_rn(fo, (float)x.x);
-      fs = __fadd_rn(fs, (float)x.y);
-      ft = __fadd_rn(ft, (float)x.z);
+  __syncthreads();
+  const int start = s_start;
+  float fo = s_f[0], fs = s_f[1], ft = s_f[2];
+  for (int s = start; s < p.S; s++) {
+    const int n = p.foldcnt[(size_t)o * p.S + s];
+    const int4* v = p.foldv + (size_t)o * p.G * p.G + (size_t)s * p.H * p.G;
+    for (int c0 = 0; c0 < n; c0 += kFoldChunk) {
+      const int m = min(kFoldChunk, n - c0);
+      __syncthreads();
+      for (int k = threadIdx.x; k < m; k += blockDim.x) stage[k] = v[c0 + k];
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        for (int k = 0; k < m; k++) {
+          const int4 x = stage[k];
+          fo = __fadd_rn(fo, (float)x.x);
+          fs = __fadd_rn(fs, (float)x.y);
+          ft = __fadd_rn(ft, (float)x.z);
+        }
+      }
     }
   }
-  p.out_vof[id] = fo; p.out_vssf[id] = fs; p.out_vtcf[id] = ft;
+  if (threadIdx.x == 0) {
+    p.out_vof[id] = fo; p.out_vssf[id] = fs; p.out_vtcf[id] = ft;
+  }
 }
 
 }  // namespace tomo
@@ -962,55 +997,75 @@ size_t strip_smem_bytes(int H, int G, int ent_cap)
 
 cudaError_t configure_kernels(size_t strip_smem)
 {
-  cudaError_t e = cudaFuncSetAttribute(k_strip, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)strip_smem);
+  return cudaFuncSetAttribute(k_strip, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)strip_smem);
+}
+
+// Launch bookkeeping: every launch is counted; with timing on, a pair of
+// events brackets it on its own stream.
+static void log_begin(LaunchLog* L, int kind, cudaStream_t s)
+{
+  if (!L) return;
+  L->launches[kind]++;
+  if (!L->timing) return;
+  cudaEvent_t a = L->take_event(), b = L->take_event();
+  cudaEventRecord(a, s);
+  L->pending.push_back({kind, a, b});
+}
+
+static void log_end(LaunchLog* L, cudaStream_t s)
+{
+  if (!L || !L->timing) return;
+  cudaEventRecord(L->pending.back().stop, s);
+}
+
+#define TOMO_LAUNCH(kind, stream, ...)  \
+  do {                                   \
+    log_begin(L, kind, stream);          \
+    __VA_ARGS__;                         \
+    log_end(L, stream);                  \
+  } while (0)
+
+static dim3 tri_grid(const EngineParams& p)
+{
+  const int b = (p.nT + 255) / 256 < 64 ? (p.nT + 255) / 256 : 64;
+  return dim3(b > 0 ? b : 1, p.Bo);
+}
+
+static dim3 vtx_grid(const EngineParams& p)
+{
+  const int b = (p.nV + 255) / 256 < 64 ? (p.nV + 255) / 256 : 64;
+  return dim3(b > 0 ? b : 1, p.Bo);
+}
+
+// Count pass of one batch (reset, rotate, bin count, bin scan).
+cudaError_t launch_bin_count(const EngineParams& p, cudaStream_t main, LaunchLog* L)
+{
+  TOMO_LAUNCH(kKReset, main, (k_reset<<<p.Bo, 256, 0, main>>>(p)));
+  TOMO_LAUNCH(kKRotate, main, (k_rotate<<<vtx_grid(p), 256, 0, main>>>(p)));
+  TOMO_LAUNCH(kKCount, main, (k_bin_count<<<tri_grid(p), 256, sizeof(int) * p.S, main>>>(p)));
+  TOMO_LAUNCH(kKScan, main, (k_bin_scan<<<p.Bo, 1024, 0, main>>>(p)));
+  return cudaGetLastError();
+}
+
+// Remainder of a batch after launch_bin_count (bin fill, strips, bed).
+cudaError_t launch_after_count(const EngineParams& p, cudaStream_t main, size_t strip_smem, LaunchLog* L)
+{
+  TOMO_LAUNCH(kKFill, main, (k_bin_fill<<<tri_grid(p), 256, 2 * sizeof(int) * p.S, main>>>(p)));
+  TOMO_LAUNCH(kKStrip, main, (k_strip<<<dim3(p.S, p.Bo), 256, strip_smem, main>>>(p)));
+  TOMO_LAUNCH(kKBed, main, (k_bed<<<dim3(8, p.Bo), 256, 0, main>>>(p)));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch(const EngineParams& p, cudaStream_t main, size_t strip_smem, LaunchLog* L)
+{
+  cudaError_t e = launch_bin_count(p, main, L);
   if (e != cudaSuccess) return e;
-  return cudaSuccess;
+  return launch_after_count(p, main, strip_smem, L);
 }
 
-// Everything of one batch except the fold; the fold goes to `side` after
-// `ready` is recorded on `main`.
-cudaError_t launch_batch(const EngineParams& p, cudaStream_t main, size_t strip_smem)
+cudaError_t launch_fold(const EngineParams& p, cudaStream_t side, LaunchLog* L)
 {
-  k_reset<<<p.Bo, 256, 0, main>>>(p);
-  const int rot_blocks = (p.nV + 255) / 256 < 64 ? (p.nV + 255) / 256 : 64;
-  k_rotate<<<dim3(rot_blocks > 0 ? rot_blocks : 1, p.Bo), 256, 0, main>>>(p);
-  const int tri_blocks = (p.nT + 255) / 256 < 64 ? (p.nT + 255) / 256 : 64;
-  const dim3 tg(tri_blocks > 0 ? tri_blocks : 1, p.Bo);
-  k_bin_count<<<tg, 256, sizeof(int) * p.S, main>>>(p);
-  k_bin_scan<<<p.Bo, 1024, 0, main>>>(p);
-  k_bin_fill<<<tg, 256, 2 * sizeof(int) * p.S, main>>>(p);
-  k_strip<<<dim3(p.S, p.Bo), 256, strip_smem, main>>>(p);
-  k_bed<<<dim3(8, p.Bo), 256, 0, main>>>(p);
-  return cudaGetLastError();
-}
-
-cudaError_t launch_fold(const EngineParams& p, cudaStream_t side)
-{
-  k_fold<<<(p.Bo + 63) / 64, 64, 0, side>>>(p);
-  return cudaGetLastError();
-}
-
-// Count pass only (safe mode sizes its bin buffer from the exact totals).
-cudaError_t launch_bin_count(const EngineParams& p, cudaStream_t main)
-{
-  k_reset<<<p.Bo, 256, 0, main>>>(p);
-  const int rot_blocks = (p.nV + 255) / 256 < 64 ? (p.nV + 255) / 256 : 64;
-  k_rotate<<<dim3(rot_blocks > 0 ? rot_blocks : 1, p.Bo), 256, 0, main>>>(p);
-  const int tri_blocks = (p.nT + 255) / 256 < 64 ? (p.nT + 255) / 256 : 64;
-  const dim3 tg(tri_blocks > 0 ? tri_blocks : 1, p.Bo);
-  k_bin_count<<<tg, 256, sizeof(int) * p.S, main>>>(p);
-  k_bin_scan<<<p.Bo, 1024, 0, main>>>(p);
-  return cudaGetLastError();
-}
-
-// Remainder of a batch after launch_bin_count.
-cudaError_t launch_after_count(const EngineParams& p, cudaStream_t main, size_t strip_smem)
-{
-  const int tri_blocks = (p.nT + 255) / 256 < 64 ? (p.nT + 255) / 256 : 64;
-  const dim3 tg(tri_blocks > 0 ? tri_blocks : 1, p.Bo);
-  k_bin_fill<<<tg, 256, 2 * sizeof(int) * p.S, main>>>(p);
-  k_strip<<<dim3(p.S, p.Bo), 256, strip_smem, main>>>(p);
-  k_bed<<<dim3(8, p.Bo), 256, 0, main>>>(p);
+  TOMO_LAUNCH(kKFold, side, (k_fold<<<p.Bo, 128, 0, side>>>(p)));
   return cudaGetLastError();
 }
 

@@ -50,6 +50,8 @@ EXPORTS = [
     ("tomoSweepDevice", ct.c_int, [ct.c_void_p, ct.c_void_p, _f32p]),
     ("tomoFinish", ct.c_int, [_f32p, _f32p, _f32p]),
     ("tomoGridSize", ct.c_int, []),
+    ("tomoProfile", ct.c_int, [ct.c_int, ct.c_int]),
+    ("tomoGetKernelLog", ct.c_int, [_i64p, ct.POINTER(ct.c_double), _i64p, ct.c_int]),
     ("tomoColumnDump", ct.c_int, [ct.c_int, ct.c_int, _i32p, _u32p, _i16p]),
 ]
 
@@ -107,6 +109,23 @@ def vol_to_mass(f32info, i32info, vm22) -> np.ndarray:
     vm = np.ascontiguousarray(vm22, np.float32).copy()
     lib().tomoVolToMass(_p(f32info, _f32p), _p(i32info, _i32p), _p(vm, _f32p))
     return vm
+
+
+KERNEL_KINDS = ("k_reset", "k_rotate", "k_bin_count", "k_bin_scan", "k_bin_fill", "k_strip", "k_bed", "k_fold")
+
+
+def profile(enable: bool, reset: bool = True) -> None:
+    """Per-launch CUDA-event timing inside the engine (events on each kernel's own stream)."""
+    lib().tomoProfile(1 if enable else 0, 1 if reset else 0)
+
+
+def kernel_log() -> dict:
+    n = len(KERNEL_KINDS)
+    launches = np.zeros(n, np.int64)
+    ms = np.zeros(n, np.float64)
+    timed = np.zeros(n, np.int64)
+    lib().tomoGetKernelLog(_p(launches, _i64p), ms.ctypes.data_as(ct.POINTER(ct.c_double)), _p(timed, _i64p), n)
+    return {k: dict(launches=int(launches[i]), ms=float(ms[i]), timed=int(timed[i])) for i, k in enumerate(KERNEL_KINDS)}
 
 
 def set_option(key: int, value: int) -> None:
