@@ -298,7 +298,8 @@ def run_ours(args, rank, world, local_rank):
                                                 "strip_h": native.stats()["strip_h"]}),
             "time_to_exact_optimum_s": total_ms / args.steps / 1000.0,
             "triangle_orientations_per_s": value * mesh.n_tri,
-            "optID": int(opt), "safe_reruns_per_step": native.stats()["safe_reruns"],
+            "optID": int(opt),
+            "reruns_per_step": {"overflow": native.stats()["overflow_reruns"], "safe": native.stats()["safe_reruns"]},
             "roofline": roof,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": int(sum(v["launches"] for v in klog.values())),

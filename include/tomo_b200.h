@@ -81,12 +81,14 @@ float tomoShadowThreshold(float theta_c);
 void tomoVolToMass(const float* f32info, const int* i32info, float* vm22);
 
 /* Tuning / test hooks. */
-#define TOMO_OPT_BATCH 1        /* orientations per device batch (default 64) */
+#define TOMO_OPT_BATCH 1        /* orientations per device batch (default 128) */
 #define TOMO_OPT_STRIP_H 2      /* force strip height 1, 2, 4 or 8 (0 = automatic) */
 #define TOMO_OPT_FORCE_SAFE 3   /* 1 = evaluate every orientation in safe mode */
+#define TOMO_OPT_NORMAL_SMEM 4  /* shared-memory bytes of a normal strip CTA (0 = 72 KB, three per SM) */
 int tomoSetOption(int key, int value);
 
-/* out[0..7] = grid edge, strip height, strips, entry capacity, safe re-runs, nYPR, batch, 0 */
+/* out[0..7] = grid edge, strip height, strips, entry capacity, orientations re-run
+ * with a large strip capacity, nYPR, batch, orientations re-run in safe mode */
 int tomoGetStats(long long* out, int n);
 
 /* Per-orientation results of the last sweep; any pointer may be null. */
@@ -103,7 +105,7 @@ int tomoSweepDevice(void* ev_start, void* ev_stop, float* kernel_ms);
 int tomoFinish(float* Mo, float* Mss, float* Vtc);
 
 /* Launch accounting.  Kernel kinds, in order: reset, rotate, bin_count,
- * bin_scan, bin_fill, strip, bed, fold.  tomoProfile(enable, reset) turns
+ * bin_scan, bin_fill, strip, bed, fold, strip re-runs.  tomoProfile(enable, reset) turns
  * per-launch CUDA-event timing on or off (events are recorded on the stream
  * each kernel is launched on) and optionally clears the log;
  * tomoGetKernelLog fills launches / total ms / timed launches per kind and

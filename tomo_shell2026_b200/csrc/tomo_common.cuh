@@ -71,6 +71,7 @@ struct EngineParams {
   int H;                // strip height in x columns
   int S;                // number of strips = ceil(G / H)
   int mode;             // 0 normal, 1 safe
+  int variant;          // strip configuration (launch accounting only)
 
   // raster constants
   float half;           // dVoxel * 0.5f
@@ -86,7 +87,7 @@ struct EngineParams {
   // work buffers
   float4* xf;           // [Bo][nV] rotated x, y, z, n.z
   unsigned* minkey;     // [Bo][4] order-preserving keys of AABB minima
-  uint8_t* tcode;       // [Bo][nT]
+  unsigned* trange;     // [Bo][nT] packed strip range of each triangle (k_bin_count -> k_bin_fill)
   int* bin_off;         // [Bo][S + 1]
   int* bin_cur;         // [Bo][S]
   int* bins;            // [Bo][bin_cap]
@@ -121,7 +122,7 @@ struct EngineParams {
 };
 
 // Kernel kinds for launch accounting.
-enum : int { kKReset = 0, kKRotate, kKCount, kKScan, kKFill, kKStrip, kKBed, kKFold, kKinds };
+enum : int { kKReset = 0, kKRotate, kKCount, kKScan, kKFill, kKStrip, kKBed, kKFold, kKStripRedo, kKinds };
 
 // Host-side launch log: launch counts per kernel kind and, when timing is
 // on, one event pair per launch recorded on the launching stream.

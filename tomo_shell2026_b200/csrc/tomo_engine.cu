@@ -26,8 +26,8 @@
 
 namespace tomo {
 
-size_t strip_smem_bytes(int H, int G, int ent_cap);
-cudaError_t configure_kernels(size_t strip_smem);
+size_t strip_smem_bytes(int mode, int H, int G, int ent_cap);
+cudaError_t configure_kernels(size_t normal_smem, size_t safe_smem);
 cudaError_t launch_batch(const EngineParams& p, cudaStream_t main, size_t strip_smem, LaunchLog* L);
 cudaError_t launch_fold(const EngineParams& p, cudaStream_t side, LaunchLog* L);
 cudaError_t launch_bin_count(const EngineParams& p, cudaStream_t main, LaunchLog* L);
@@ -198,7 +198,7 @@ struct Engine {
   // batch work buffers
   DevBuf<float4> xf;
   DevBuf<unsigned> minkey;
-  DevBuf<uint8_t> tcode;
+  DevBuf<unsigned> trange;
   DevBuf<int> bin_off, bin_cur, bins, bbox;
   DevBuf<uint8_t> bedf;
   BatchSet set[2];
@@ -214,9 +214,10 @@ struct Engine {
   // host results of the last sweep
   Params P{};
   int nYPR = 0, G = 0, H = 0, S = 0, ent_cap = 0;
-  int batch = 64;
+  int batch = 128;
   int force_h = 0;        // test hook: strip height override
   int force_safe = 0;     // test hook: run every orientation in safe mode
+  int normal_smem = 0;    // shared-memory budget of a normal strip CTA (0 = 72 KB)
   float cx = 0, cy = 0, cz = 0;
   std::vector<float> h_rot;
   std::vector<long long> vo64, vss64, vtc64, entries, columns;
@@ -226,6 +227,7 @@ struct Engine {
   float mat4x4[16] = {0};
   double last_kernel_ms = 0.0;
   int n_safe = 0;
+  int n_redo[4] = {0, 0, 0, 0};
   int H_sweep = 0;        // strip height of the last normal sweep
   LaunchLog log;
 
@@ -248,7 +250,7 @@ struct Engine {
   void release()
   {
     vpos.release(); vnrm.release(); tri.release(); rot.release(); ori.release();
-    xf.release(); minkey.release(); tcode.release(); bin_off.release(); bin_cur.release(); bins.release();
+    xf.release(); minkey.release(); trange.release(); bin_off.release(); bin_cur.release(); bins.release();
     bbox.release(); bedf.release();
     for (auto& s : set) { s.acc.release(); s.flags.release(); s.foldcnt.release(); s.foldv.release(); s.foldmeta.release(); }
     o_vo.release(); o_vss.release(); o_vtc.release(); o_ent.release(); o_col.release();
@@ -277,28 +279,56 @@ struct Engine {
     return (int)span + (int)std::max(0.0f, P.bed_outer) + 2;
   }
 
-  void choose_strips(int mode)
+  // Strip configurations.
+  //   0 normal     : H0-column strips, ~72 KB of shared memory (three CTAs
+  //                  per SM), entries without priorities; H0 is the tallest
+  //                  strip with room for two entries per slot;
+  //   1 safe       : H0-column strips, whole-box evaluation, priorities,
+  //                  all opt-in shared memory;
+  //   2 big normal : configuration 0 semantics with all opt-in shared memory
+  //                  (orientations whose strip lists overflowed);
+  //   3 narrow safe: safe mode with one-column strips (last resort).
+  struct StripCfg { int H, S, C; size_t smem; int mode; };
+  StripCfg cfg[4];
+
+  void plan_strips()
   {
-    const size_t budget = std::min<size_t>(smem_optin ? smem_optin : 232448, 110 * 1024);
-    if (mode == 1) {
-      H = 1;
-      S = G;
-      size_t fixed = strip_smem_bytes(1, G, 0);
-      ent_cap = (int)((std::min<size_t>(smem_optin ? smem_optin : 232448, 220 * 1024) - fixed) / 17);
-      return;
-    }
-    int best_h = 1;
+    const size_t optin = smem_optin ? smem_optin : 232448;
+    const size_t budget0 = std::min<size_t>(optin - 2048, normal_smem ? (size_t)normal_smem : 73728);
+    // the strip kernel also holds ~0.7 KB of static shared memory
+    const size_t budget1 = std::min<size_t>(optin, 227 * 1024) - 2048;
+    int h0 = 1;
     for (int h : {8, 4, 2, 1}) {
       if (force_h && h != force_h) continue;
-      const size_t fixed = strip_smem_bytes(h, G, 0);
-      if (fixed >= budget) continue;
-      const int cap = (int)((budget - fixed) / 17);
-      if (force_h || cap >= (5 * h * G) / 4) { best_h = h; break; }
+      const size_t fixed = strip_smem_bytes(0, h, G, 0);
+      if (fixed + 6 * 256 >= budget0) continue;
+      const int cap = (int)std::min<size_t>((budget0 - fixed) / 6 - 16, 32767);
+      if (force_h || cap >= 2 * h * G) { h0 = h; break; }
     }
-    H = best_h;
-    S = (G + H - 1) / H;
-    const size_t fixed = strip_smem_bytes(H, G, 0);
-    ent_cap = (int)((budget > fixed ? budget - fixed : 0) / 17);
+    auto make = [&](int mode, int h, size_t budget) {
+      StripCfg c;
+      c.mode = mode; c.H = h; c.S = (G + h - 1) / h;
+      const size_t per = mode == 0 ? 6 : 15;
+      const size_t fixed = strip_smem_bytes(mode, h, G, 0);
+      c.C = (int)std::min<size_t>(budget > fixed + 32 * per ? (budget - fixed) / per - 16 : 16, 32767);
+      c.smem = strip_smem_bytes(mode, h, G, c.C);
+      return c;
+    };
+    cfg[0] = make(0, h0, budget0);
+    cfg[1] = make(1, h0, budget1);
+    cfg[2] = make(0, h0, budget1);
+    cfg[3] = make(1, 1, budget1);
+  }
+
+  void choose_strips(int c)
+  {
+    H = cfg[c].H; S = cfg[c].S; ent_cap = cfg[c].C;
+  }
+
+  int configure()
+  {
+    TOMO_CUDA(configure_kernels(std::max(cfg[0].smem, cfg[2].smem), std::max(cfg[1].smem, cfg[3].smem)));
+    return 0;
   }
 
   int upload(const float* f32, const int* i32, const float* ypr, const int* tri_h, const float* vtx,
@@ -332,6 +362,7 @@ struct Engine {
     cz = (float)((double)(mn[2] + mx[2]) * 0.5);
     G = choose_grid(vtx, P.n_vtx);
     if (G > kMaxGrid) return set_error(TOMO_ERR_CAPACITY, "mesh extent exceeds the supported slot grid");
+    plan_strips();
 
     std::vector<float4> hp(std::max(P.n_vtx, 1)), hn(std::max(P.n_vtx, 1));
     for (int v = 0; v < P.n_vtx; v++) {
@@ -385,7 +416,7 @@ struct Engine {
     const size_t GG = (size_t)G * G;
     TOMO_CUDA(xf.reserve((size_t)Bo * std::max(P.n_vtx, 1)));
     TOMO_CUDA(minkey.reserve((size_t)Bo * 4));
-    TOMO_CUDA(tcode.reserve((size_t)Bo * std::max(P.n_tri, 1)));
+    TOMO_CUDA(trange.reserve((size_t)Bo * std::max(P.n_tri, 1)));
     TOMO_CUDA(bin_off.reserve((size_t)Bo * (S + 1)));
     TOMO_CUDA(bin_cur.reserve((size_t)Bo * S));
     TOMO_CUDA(bins.reserve((size_t)Bo * bin_cap));
@@ -415,25 +446,22 @@ struct Engine {
   {
     p.Bo = Bo;
     p.ori = ori.ptr + first;
-    p.xf = xf.ptr; p.minkey = minkey.ptr; p.tcode = tcode.ptr;
+    p.xf = xf.ptr; p.minkey = minkey.ptr; p.trange = trange.ptr;
     p.bin_off = bin_off.ptr; p.bin_cur = bin_cur.ptr; p.bins = bins.ptr; p.bin_cap = bin_cap;
     p.bbox = bbox.ptr; p.bedf = bedf.ptr;
     p.acc = set[which].acc.ptr; p.flags = set[which].flags.ptr;
     p.foldcnt = set[which].foldcnt.ptr; p.foldv = set[which].foldv.ptr; p.foldmeta = set[which].foldmeta.ptr;
   }
 
-  // All orientations in normal mode (or safe mode when forced), asynchronously on `main`.
+  // All orientations in configuration 0, asynchronously on `main`.
   int sweep_device()
   {
     if (nYPR == 0 || P.n_tri == 0) return 0;
-    const int mode = force_safe ? 1 : 0;
-    choose_strips(mode);
+    choose_strips(0);
     H_sweep = H;
-    const size_t smem = strip_smem_bytes(H, G, ent_cap);
-    TOMO_CUDA(configure_kernels(smem));
+    TOMO_TRY(configure());
     const int Bo = std::min(batch, nYPR);
-    const int bin_cap = mode == 0 ? 4 * P.n_tri + 4096 : 0;
-    if (mode == 1) return run_safe_all();
+    const int bin_cap = 4 * P.n_tri + 4096;
     TOMO_TRY(reserve_outputs());
     TOMO_TRY(reserve_batch(Bo, bin_cap));
     TOMO_CUDA(cudaMemsetAsync(o_nbed.ptr, 0, sizeof(int) * nYPR, main));
@@ -444,7 +472,7 @@ struct Engine {
       const int which = k & 1;
       if (k >= 2) TOMO_CUDA(cudaStreamWaitEvent(main, set[which].folded, 0));
       bind_batch(p, nb, bin_cap, which, first);
-      TOMO_CUDA(launch_batch(p, main, smem, &log));
+      TOMO_CUDA(launch_batch(p, main, cfg[0].smem, &log));
       TOMO_CUDA(cudaEventRecord(ev_ready, main));
       TOMO_CUDA(cudaStreamWaitEvent(side, ev_ready, 0));
       TOMO_CUDA(launch_fold(p, side, &log));
@@ -456,51 +484,50 @@ struct Engine {
     return 0;
   }
 
-  // Safe mode for a list of orientation ids (host-synchronous: the bin
-  // buffer is sized from the exact counts).
-  int run_safe(const std::vector<int>& ids)
+  // Re-run a list of orientation ids in configuration c (host-synchronous).
+  int run_subset(const std::vector<int>& ids, int c)
   {
     if (ids.empty()) return 0;
-    choose_strips(1);
-    const size_t smem = strip_smem_bytes(H, G, ent_cap);
-    TOMO_CUDA(configure_kernels(smem));
+    choose_strips(c);
+    const int mode = cfg[c].mode;
+    TOMO_TRY(configure());
     TOMO_TRY(reserve_outputs());
+    TOMO_CUDA(cudaStreamSynchronize(side));
     DevBuf<int> sub;
     TOMO_CUDA(sub.reserve(ids.size()));
     TOMO_CUDA(cudaMemcpyAsync(sub.ptr, ids.data(), sizeof(int) * ids.size(), cudaMemcpyHostToDevice, main));
     const int Bo = std::min<int>(batch, (int)ids.size());
-    TOMO_TRY(reserve_batch(Bo, 1));
-    EngineParams p = base_params(1);
+    const int normal_cap = 4 * P.n_tri + 4096;
+    TOMO_TRY(reserve_batch(Bo, mode == 0 ? normal_cap : 1));
+    EngineParams p = base_params(mode);
+    p.variant = c;
     for (int first = 0; first < (int)ids.size(); first += Bo) {
       const int nb = std::min<int>(Bo, (int)ids.size() - first);
-      // The count pass decides the bin capacity, so it runs without one.
-      bind_batch(p, nb, INT_MAX, 0, 0);
-      p.ori = sub.ptr + first;
-      TOMO_CUDA(launch_bin_count(p, main, &log));
-      std::vector<int> off((size_t)nb * (S + 1));
-      TOMO_CUDA(cudaMemcpyAsync(off.data(), bin_off.ptr, sizeof(int) * off.size(), cudaMemcpyDeviceToHost, main));
-      TOMO_CUDA(cudaStreamSynchronize(main));
-      int cap = 1;
-      for (int o = 0; o < nb; o++) cap = std::max(cap, off[(size_t)o * (S + 1) + S]);
-      TOMO_CUDA(bins.reserve((size_t)nb * cap));
-      p.bins = bins.ptr; p.bin_cap = cap;
       for (int o = 0; o < nb; o++) TOMO_CUDA(cudaMemsetAsync(o_nbed.ptr + ids[first + o], 0, sizeof(int), main));
-      TOMO_CUDA(launch_after_count(p, main, smem, &log));
+      if (mode == 0) {
+        bind_batch(p, nb, normal_cap, 0, 0);
+        p.ori = sub.ptr + first;
+        TOMO_CUDA(launch_batch(p, main, cfg[c].smem, &log));
+      } else {
+        // the count pass decides the bin capacity, so it runs without one
+        bind_batch(p, nb, INT_MAX, 0, 0);
+        p.ori = sub.ptr + first;
+        TOMO_CUDA(launch_bin_count(p, main, &log));
+        std::vector<int> off((size_t)nb * (S + 1));
+        TOMO_CUDA(cudaMemcpyAsync(off.data(), bin_off.ptr, sizeof(int) * off.size(), cudaMemcpyDeviceToHost, main));
+        TOMO_CUDA(cudaStreamSynchronize(main));
+        int cap = 1;
+        for (int o = 0; o < nb; o++) cap = std::max(cap, off[(size_t)o * (S + 1) + S]);
+        TOMO_CUDA(bins.reserve((size_t)nb * cap));
+        p.bins = bins.ptr; p.bin_cap = cap;
+        TOMO_CUDA(launch_after_count(p, main, cfg[c].smem, &log));
+      }
       TOMO_CUDA(launch_fold(p, main, &log));
-      TOMO_CUDA(cudaStreamSynchronize(main));
     }
+    TOMO_CUDA(cudaStreamSynchronize(main));
     sub.release();
-    n_safe += (int)ids.size();
+    n_redo[c] += (int)ids.size();
     return 0;
-  }
-
-  int run_safe_all()
-  {
-    std::vector<int> ids(nYPR);
-    for (int i = 0; i < nYPR; i++) ids[i] = i;
-    TOMO_TRY(reserve_outputs());
-    TOMO_CUDA(cudaMemsetAsync(o_nbed.ptr, 0, sizeof(int) * nYPR, main));
-    return run_safe(ids);
   }
 
   int fetch()
@@ -525,31 +552,50 @@ struct Engine {
     return 0;
   }
 
-  // Full device phase: normal sweep, then safe re-runs of flagged orientations.
+  // Full device phase: the sweep in configuration 0, then the re-runs of
+  // flagged orientations: overflowed strip lists in configuration 2, stray
+  // hits and priority-dependent columns in configuration 1, and what still
+  // overflows in configuration 3.
   int execute()
   {
-    n_safe = 0;
-    int rc = sweep_device();
-    if (rc) return rc;
-    rc = fetch();
-    if (rc) return rc;
-    std::vector<int> redo;
-    for (int i = 0; i < nYPR; i++) {
-      if (flags[i] & kFlagGrid) return set_error(TOMO_ERR_CAPACITY, "slot index outside the grid");
-      if (flags[i] & (kFlagStray | kFlagOverflow | kFlagBinCap)) redo.push_back(i);
+    for (int& r : n_redo) r = 0;
+    std::vector<int> big, safe, narrow;
+    if (force_safe) {
+      if (nYPR == 0 || P.n_tri == 0) return fetch();
+      TOMO_TRY(reserve_outputs());
+      for (int i = 0; i < nYPR; i++) safe.push_back(i);
+    } else {
+      TOMO_TRY(sweep_device());
+      TOMO_TRY(fetch());
+      for (int i = 0; i < nYPR; i++) {
+        if (flags[i] & kFlagGrid) return set_error(TOMO_ERR_CAPACITY, "slot index outside the grid");
+        if (flags[i] & (kFlagStray | kFlagBinCap)) safe.push_back(i);
+        else if (flags[i] & kFlagOverflow) big.push_back(i);
+      }
+      if (!big.empty()) {
+        TOMO_TRY(run_subset(big, 2));
+        TOMO_TRY(fetch());
+        for (int id : big)
+          if (flags[id] & (kFlagStray | kFlagBinCap | kFlagOverflow)) safe.push_back(id);
+      }
     }
-    if (!redo.empty()) {
-      rc = run_safe(redo);
-      if (rc) return rc;
-      rc = fetch();
-      if (rc) return rc;
+    if (!safe.empty()) {
+      TOMO_TRY(run_subset(safe, 1));
+      TOMO_TRY(fetch());
+      for (int id : safe)
+        if (flags[id] & kFlagSafeOverflow) narrow.push_back(id);
+    }
+    if (!narrow.empty()) {
+      TOMO_TRY(run_subset(narrow, 3));
+      TOMO_TRY(fetch());
     }
     for (int i = 0; i < nYPR; i++) {
       if (flags[i] & kFlagSafeOverflow) return set_error(TOMO_ERR_CAPACITY, "column strip exceeds shared memory");
       if (flags[i] & kFlagGrid) return set_error(TOMO_ERR_CAPACITY, "slot index outside the grid");
       if (flags[i] & (kFlagStray | kFlagOverflow | kFlagBinCap))
-        return set_error(TOMO_ERR_CAPACITY, "orientation unresolved after the safe re-run");
+        return set_error(TOMO_ERR_CAPACITY, "orientation unresolved after the re-runs");
     }
+    n_safe = n_redo[1] + n_redo[2] + n_redo[3];
     return 0;
   }
 
@@ -559,8 +605,8 @@ struct Engine {
     if (id < 0 || id >= nYPR) return set_error(TOMO_ERR_ARG, "orientation index out of range");
     if (P.n_tri == 0) return set_error(TOMO_ERR_ARG, "empty mesh");
     choose_strips(mode);
-    const size_t smem = strip_smem_bytes(H, G, ent_cap);
-    TOMO_CUDA(configure_kernels(smem));
+    const size_t smem = cfg[mode].smem;
+    TOMO_TRY(configure());
     TOMO_TRY(reserve_outputs());
     const size_t GG = (size_t)G * G;
     TOMO_CUDA(dump_cols.reserve(GG * 8)); TOMO_CUDA(dump_keys.reserve(GG * 64)); TOMO_CUDA(dump_types.reserve(GG * 64));
@@ -746,6 +792,7 @@ int tomoSetOption(int key, int value)
     case TOMO_OPT_BATCH: if (value < 1) return TOMO_ERR_ARG; E.batch = value; return 0;
     case TOMO_OPT_STRIP_H: if (value < 0 || value > 8) return TOMO_ERR_ARG; E.force_h = value; return 0;
     case TOMO_OPT_FORCE_SAFE: E.force_safe = value ? 1 : 0; return 0;
+    case TOMO_OPT_NORMAL_SMEM: if (value < 0 || value > 232448) return TOMO_ERR_ARG; E.normal_smem = value; return 0;
     default: return TOMO_ERR_ARG;
   }
 }
@@ -756,7 +803,7 @@ int tomoGetStats(long long* out, int n)
   if (!g_engine || out == nullptr) return TOMO_ERR_ARG;
   const Engine& E = *g_engine;
   const long long v[8] = {E.G, E.H_sweep, (E.G + std::max(E.H_sweep, 1) - 1) / std::max(E.H_sweep, 1),
-                          E.ent_cap, E.n_safe, E.nYPR, E.batch, 0};
+                          E.cfg[0].C, E.n_redo[2], E.nYPR, E.batch, E.n_redo[1] + E.n_redo[3]};
   for (int i = 0; i < n && i < 8; i++) out[i] = v[i];
   return 0;
 }

@@ -222,6 +222,7 @@ __global__ void k_reset(EngineParams p)
   if (threadIdx.x < 4) p.minkey[o * 4 + threadIdx.x] = f2key(1e5f);  // STomoAABB3Df::Init
   for (int s = threadIdx.x; s <= p.S; s += blockDim.x) p.bin_off[(size_t)o * (p.S + 1) + s] = 0;
   for (int s = threadIdx.x; s < p.S; s += blockDim.x) { p.bin_cur[(size_t)o * p.S + s] = 0; p.foldcnt[(size_t)o * p.S + s] = 0; }
+  for (int s = threadIdx.x; s < p.S * 8; s += blockDim.x) p.foldmeta[(size_t)o * p.S * 8 + s] = 0;
 }
 
 // ---------------------------------------------------------------- K1 rotate
@@ -313,6 +314,19 @@ __device__ __forceinline__ BinRange bin_range(const EngineParams& p, int o, int 
   return r;
 }
 
+// Packed strip range of one (orientation, triangle): s0 | s1 << 12 | code << 24.
+__device__ __forceinline__ unsigned pack_range(const BinRange& r)
+{
+  return (unsigned)r.s0 | ((unsigned)r.s1 << 12) | ((unsigned)r.code << 24);
+}
+
+__device__ __forceinline__ BinRange unpack_range(unsigned v)
+{
+  BinRange r;
+  r.s0 = (int)(v & 0xFFFu); r.s1 = (int)((v >> 12) & 0xFFFu); r.code = (int)(v >> 24);
+  return r;
+}
+
 __global__ void __launch_bounds__(256) k_bin_count(EngineParams p)
 {
   extern __shared__ int sh_cnt[];
@@ -322,9 +336,14 @@ __global__ void __launch_bounds__(256) k_bin_count(EngineParams p)
   if (threadIdx.x == 0) sflag = 0;
   __syncthreads();
   const Shift sh = load_shift(p, o);
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < p.nT; t += gridDim.x * blockDim.x) {
-    const BinRange r = bin_range(p, o, t, sh, &sflag, nullptr);
-    p.tcode[(size_t)o * p.nT + t] = (uint8_t)r.code;
+  const int stride = gridDim.x * blockDim.x;
+  for (int tb = blockIdx.x * blockDim.x; tb < p.nT; tb += stride) {   // warp-uniform trip count
+    const int t = tb + threadIdx.x;
+    BinRange r; r.s0 = 0; r.s1 = -1; r.code = 0;
+    if (t < p.nT) {
+      r = bin_range(p, o, t, sh, &sflag, nullptr);
+      p.trange[(size_t)o * p.nT + t] = pack_range(r);
+    }
     for (int s = r.s0; s <= r.s1; s++) atomicAdd(&sh_cnt[s], 1);
   }
   __syncthreads();
@@ -372,16 +391,15 @@ __global__ void __launch_bounds__(256) k_bin_fill(EngineParams p)
   extern __shared__ int sh_fill[];
   int* lc = sh_fill;            // [S]
   int* base = sh_fill + p.S;    // [S]
-  __shared__ int sflag;
   const int o = blockIdx.y;
   for (int s = threadIdx.x; s < p.S; s += blockDim.x) lc[s] = 0;
-  if (threadIdx.x == 0) sflag = 0;
   __syncthreads();
-  const Shift sh = load_shift(p, o);
   const int stride = gridDim.x * blockDim.x;
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < p.nT; t += stride) {
-    const uint8_t code = p.tcode[(size_t)o * p.nT + t];
-    const BinRange r = bin_range(p, o, t, sh, &sflag, &code);
+  const unsigned* tr = p.trange + (size_t)o * p.nT;
+  for (int tb = blockIdx.x * blockDim.x; tb < p.nT; tb += stride) {
+    const int t = tb + threadIdx.x;
+    BinRange r; r.s0 = 0; r.s1 = -1; r.code = 0;
+    if (t < p.nT) r = unpack_range(tr[t]);
     for (int s = r.s0; s <= r.s1; s++) atomicAdd(&lc[s], 1);
   }
   __syncthreads();
@@ -392,9 +410,10 @@ __global__ void __launch_bounds__(256) k_bin_fill(EngineParams p)
   __syncthreads();
   const int* off = p.bin_off + (size_t)o * (p.S + 1);
   int* bins = p.bins + (size_t)o * p.bin_cap;
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < p.nT; t += stride) {
-    const uint8_t code = p.tcode[(size_t)o * p.nT + t];
-    const BinRange r = bin_range(p, o, t, sh, &sflag, &code);
+  for (int tb = blockIdx.x * blockDim.x; tb < p.nT; tb += stride) {
+    const int t = tb + threadIdx.x;
+    BinRange r; r.s0 = 0; r.s1 = -1; r.code = 0;
+    if (t < p.nT) r = unpack_range(tr[t]);
     for (int s = r.s0; s <= r.s1; s++) {
       const int pos = off[s] + base[s] + atomicAdd(&lc[s], 1);
       if (pos < p.bin_cap) bins[pos] = t | ((r.code == 2) ? (int)0x80000000 : 0);
@@ -403,25 +422,52 @@ __global__ void __launch_bounds__(256) k_bin_fill(EngineParams p)
 }
 
 // ---------------------------------------------------------------- K3 strip
+//
+// One CTA per (orientation, strip).  Normal mode keeps per entry only the
+// packed (z, nz) key and the next index (6 bytes) so four CTAs fit on an SM;
+// a column whose distinct keys exceed the 63-pixel cap needs first-come
+// priorities and sends its orientation to safe mode, which also stores the
+// (triangle, pixel, twin) priority of every entry.
 
-constexpr int kChunk = 256;   // triangles staged per pass (== blockDim.x)
+constexpr int kChunk = 256;    // triangles staged per pass (== blockDim.x)
+constexpr int kRegKeys = 8;    // columns with up to this many raw pixels sort in registers
+constexpr int kMaxEnt = 32767; // entry indices are stored as int16
 
 struct StripSmem {
-  int* heads;        // [H*G]
-  unsigned* ekey;    // [C]
-  unsigned* et;      // [C]
-  unsigned* elo;     // [C]
-  int* enext;        // [C]
-  uint8_t* emark;    // [C]
-  // triangle chunk
-  float4* q0; float4* q1; float4* q2; float4* q3; float4* q4;   // [kChunk]
-  int4* tm;          // [kChunk] t, x0, y0, ylen
-  int4* tm2;         // [kChunk] xc0, npix, kind, 0
-  int* pref;         // [kChunk + 1]
-  int* thit;         // [kChunk]
-  // per-slot results (aliases the chunk area after rasterization)
-  int* rvo; int* rvss; int* rtc;
+  int* heads;          // [H*G] first entry of each column list, -1 if empty
+  unsigned* occ;       // [ceil(H*G/32)] occupied-slot bitmap
+  unsigned* ekey;      // [C] (z+32768) << 16 | (nz+32768)
+  short* enext;        // [C] next entry of the same column, -1 at the end
+  unsigned* et;        // [C] safe mode: triangle index (priority, major)
+  unsigned* elo;       // [C] safe mode: pixel index * 2 + twin (priority, minor)
+  uint8_t* emark;      // [C] safe mode: first-come marks
+  float4* q0; float4* q1; float4* q2;   // [kChunk] margined vertices, vertex-normal z
+  float4* q3;          // [kChunk] centroid fallback position (x, y, z)
+  int4* tm;            // [kChunk] t, x0, y0, ylen
+  int2* tm2;           // [kChunk] xc0, kind
+  int* pref;           // [kChunk + 4]
+  int* thit;           // [kChunk]
+  short* olist;        // [H*G] occupied local slots in slot order (aliases the chunk area)
 };
+
+__host__ __device__ inline size_t strip_chunk_bytes()
+{
+  return 4 * sizeof(float4) * kChunk + sizeof(int4) * kChunk + sizeof(int2) * kChunk + sizeof(int) * (2 * kChunk + 4);
+}
+
+__host__ __device__ inline size_t round16(size_t b) { return (b + 15) / 16 * 16; }
+
+// Shared-memory bytes of one strip CTA (mirrors the carve-up in k_strip).
+__host__ __device__ inline size_t strip_smem_layout(int mode, int H, int G, int C)
+{
+  const size_t HG = (size_t)H * G;
+  size_t b = round16(sizeof(int) * HG) + round16(sizeof(unsigned) * ((HG + 31) / 32));
+  b += round16(sizeof(unsigned) * (size_t)C) + round16(sizeof(short) * (size_t)C);
+  if (mode == 1) b += 2 * round16(sizeof(unsigned) * (size_t)C) + round16((size_t)C);
+  const size_t chunk = strip_chunk_bytes();
+  const size_t olist = round16(sizeof(short) * HG);
+  return b + (chunk > olist ? chunk : olist);
+}
 
 struct ColState {
   int started, ex, im, tc_done;
@@ -490,56 +536,114 @@ __device__ __forceinline__ bool prio_less(unsigned ta, unsigned la, unsigned tb,
 
 struct ColOut { int vo, vss, tc, ndist, nfin, lastz, lasttype, has10; };
 
-__device__ void dump_key(const EngineParams& p, int gslot, int i, unsigned key, int type);
+__device__ __forceinline__ void dump_key(const EngineParams& p, int gslot, int i, unsigned key, int type)
+{
+  if (p.dump_keys == nullptr || i >= 64) return;
+  p.dump_keys[(size_t)gslot * 64 + i] = key;
+  p.dump_types[(size_t)gslot * 64 + i] = (short)type;
+}
+
+__device__ __forceinline__ void col_result(const EngineParams& p, ColState& s, int ndist, ColOut& r)
+{
+  r.ndist = ndist;
+  r.nfin = col_finish(s);
+  r.vo = (s.al > s.be) ? (s.al - s.be) : 0;
+  r.vss = p.explicit_ss ? (s.ssb - s.ssa) : (-s.al + s.be + s.tc - s.nvb + s.nva);
+  r.tc = s.tc;
+  r.lastz = s.lastz; r.lasttype = s.lasttype; r.has10 = s.has10;
+}
 
 // Column stage of one slot from its shared-memory list.
-__device__ ColOut column(const EngineParams& p, const StripSmem& sm, int head, bool dump, int gslot)
+template <int MODE>
+__device__ ColOut column(const EngineParams& p, const StripSmem& sm, int head, bool dump, int gslot, int* sflag)
 {
   ColOut r;
   r.vo = r.vss = r.tc = 0; r.ndist = 0; r.nfin = 0; r.lastz = 0; r.lasttype = 0; r.has10 = 0;
   if (head < 0) return r;
-  int n = 0;
-  for (int e = head; e >= 0 && n <= 16; e = sm.enext[e]) n++;
   ColState s;
   col_init(s);
-  if (n <= 16) {
-    unsigned k[16];
+  const unsigned k0 = sm.ekey[head];
+  const int e1 = sm.enext[head];
+  unsigned k1 = k0;
+  bool two = false;
+  if (e1 >= 0) {
+    k1 = sm.ekey[e1];
+    two = sm.enext[e1] < 0;
+  }
+  if (e1 < 0 || (two && k1 == k0)) {   // a single distinct pixel: no pairing
+    r.ndist = 1; r.nfin = 1; r.lastz = key_z(k0); r.lasttype = 0;
+    r.has10 = (key_z(k0) == 1 && key_nz(k0) == 0);
+    if (dump) dump_key(p, gslot, 0, k0, 0);
+    return r;
+  }
+  if (two) {                            // the common alpha/beta pair
+    const unsigned hi = (k0 > k1) ? k0 : k1, lo = (k0 > k1) ? k1 : k0;
+    const int t0 = col_step(s, key_z(hi), key_nz(hi), p.thr, p.explicit_ss);
+    const int t1 = col_step(s, key_z(lo), key_nz(lo), p.thr, p.explicit_ss);
+    if (dump) { dump_key(p, gslot, 0, hi, t0); dump_key(p, gslot, 1, lo, t1); }
+    col_result(p, s, 2, r);
+    return r;
+  }
+  int n = 0;
+  for (int e = head; e >= 0 && n <= kRegKeys; e = sm.enext[e]) n++;
+  if (n <= kRegKeys) {
+    unsigned k[kRegKeys];
     int m = 0;
 #pragma unroll
-    for (int i = 0; i < 16; i++) k[i] = 0u;
+    for (int i = 0; i < kRegKeys; i++) k[i] = 0u;
     for (int e = head; e >= 0; e = sm.enext[e]) {
       const unsigned key = sm.ekey[e];
       bool dup = false;
 #pragma unroll
-      for (int i = 0; i < 16; i++) dup |= (i < m) && (k[i] == key);
+      for (int i = 0; i < kRegKeys; i++) dup |= (i < m) && (k[i] == key);
       if (!dup) {
         unsigned cur = key;
 #pragma unroll
-        for (int i = 0; i < 16; i++) {
+        for (int i = 0; i < kRegKeys; i++) {
           if (i < m) { const unsigned a = k[i]; const bool sw = cur > a; k[i] = sw ? cur : a; cur = sw ? a : cur; }
           else if (i == m) k[i] = cur;
         }
         m++;
       }
     }
-    r.ndist = m;
     if (m == 1) {
-      r.nfin = 1; r.lastz = key_z(k[0]); r.lasttype = 0; r.has10 = (key_z(k[0]) == 1 && key_nz(k[0]) == 0);
+      r.ndist = 1; r.nfin = 1; r.lastz = key_z(k[0]); r.lasttype = 0;
+      r.has10 = (key_z(k[0]) == 1 && key_nz(k[0]) == 0);
       if (dump) dump_key(p, gslot, 0, k[0], 0);
       return r;
     }
 #pragma unroll
-    for (int i = 0; i < 16; i++) {
+    for (int i = 0; i < kRegKeys; i++) {
       if (i < m) {
         const int t = col_step(s, key_z(k[i]), key_nz(k[i]), p.thr, p.explicit_ss);
         if (dump) dump_key(p, gslot, i, k[i], t);
       }
     }
+    col_result(p, s, m, r);
+    return r;
+  }
+  int d = 0;
+  if (MODE == 0) {
+    // Long list, no priorities: visit the distinct keys in descending order.
+    // Past 63 distinct keys the first-come cap decides which survive, which
+    // needs priorities: hand the orientation to safe mode.
+    unsigned long long prev = 0x100000000ull;
+    for (;;) {
+      unsigned best = 0; bool found = false;
+      for (int e = head; e >= 0; e = sm.enext[e]) {
+        const unsigned key = sm.ekey[e];
+        if ((unsigned long long)key < prev && (!found || key > best)) { best = key; found = true; }
+      }
+      if (!found) break;
+      if (d == kSlotCap) { atomicOr(sflag, kFlagStray); return r; }
+      const int t = col_step(s, key_z(best), key_nz(best), p.thr, p.explicit_ss);
+      if (dump) dump_key(p, gslot, d, best, t);
+      prev = best;
+      d++;
+    }
   } else {
-    // Long list: first-come dedup and the 63-pixel cap need the priorities.
     // A pixel is kept iff it is the first (lowest priority) entry of its key
     // and fewer than 63 such first entries precede it (SetBit semantics).
-    int d = 0;
     for (int e = head; e >= 0; e = sm.enext[e]) {
       bool rep = true;
       for (int f = head; f >= 0; f = sm.enext[f])
@@ -557,17 +661,8 @@ __device__ ColOut column(const EngineParams& p, const StripSmem& sm, int head, b
       }
       d = kSlotCap;
     }
-    r.ndist = d;
-    if (d == 1) {
-      for (int e = head; e >= 0; e = sm.enext[e])
-        if (sm.emark[e] == 1) {
-          r.nfin = 1; r.lastz = key_z(sm.ekey[e]); r.has10 = (r.lastz == 1 && key_nz(sm.ekey[e]) == 0);
-          if (dump) dump_key(p, gslot, 0, sm.ekey[e], 0);
-          break;
-        }
-      return r;
-    }
     unsigned long long prev = 0x100000000ull;
+    int got = 0;
     for (int i = 0; i < d; i++) {
       int best = -1;
       for (int e = head; e >= 0; e = sm.enext[e])
@@ -576,21 +671,17 @@ __device__ ColOut column(const EngineParams& p, const StripSmem& sm, int head, b
       const int t = col_step(s, key_z(sm.ekey[best]), key_nz(sm.ekey[best]), p.thr, p.explicit_ss);
       if (dump) dump_key(p, gslot, i, sm.ekey[best], t);
       prev = sm.ekey[best];
+      got++;
     }
+    d = got;
   }
-  r.nfin = col_finish(s);
-  r.vo = (s.al > s.be) ? (s.al - s.be) : 0;
-  r.vss = p.explicit_ss ? (s.ssb - s.ssa) : (-s.al + s.be + s.tc - s.nvb + s.nva);
-  r.tc = s.tc;
-  r.lastz = s.lastz; r.lasttype = s.lasttype; r.has10 = s.has10;
+  if (d == 1) {   // duplicates of a single key
+    r.ndist = 1; r.nfin = 1; r.lastz = s.lastz; r.lasttype = 0; r.has10 = s.has10;
+    if (dump && p.dump_types) p.dump_types[(size_t)gslot * 64] = 0;
+    return r;
+  }
+  col_result(p, s, d, r);
   return r;
-}
-
-__device__ void dump_key(const EngineParams& p, int gslot, int i, unsigned key, int type)
-{
-  if (p.dump_keys == nullptr || i >= 64) return;
-  p.dump_keys[(size_t)gslot * 64 + i] = key;
-  p.dump_types[(size_t)gslot * 64 + i] = (short)type;
 }
 
 // Bed bookkeeping of one slot (GenerateBed, STomoSh_INT3.cpp:1414-1430).
@@ -613,20 +704,59 @@ __device__ __forceinline__ uint8_t bed_flags(const EngineParams& p, const ColOut
   return f;
 }
 
+// Append one pixel to its column list.  Entry slots are allocated once per
+// warp (ballot + popc) instead of one shared atomic per pixel.
+template <int MODE>
 __device__ __forceinline__ void emit(const EngineParams& p, const StripSmem& sm, int* nent, int* sflag,
                                      int xs0, int xs1, int sx, int sy, int z, int nz, unsigned t, unsigned lo)
 {
-  if (sx < 0 || sx >= p.G || sy < 0 || sy >= p.G) { atomicOr(sflag, kFlagGrid); return; }
-  if (sx < xs0 || sx >= xs1) { if (p.mode == 0) atomicOr(sflag, kFlagStray); return; }
-  const int e = atomicAdd(nent, 1);
-  if (e >= p.ent_cap) { atomicOr(sflag, p.mode == 0 ? kFlagOverflow : kFlagSafeOverflow); return; }
+  int bad = 0;
+  if (sx < 0 || sx >= p.G || sy < 0 || sy >= p.G) bad = kFlagGrid;
+  else if (sx < xs0 || sx >= xs1) bad = (MODE == 0) ? kFlagStray : -1;
+  const unsigned mask = __ballot_sync(__activemask(), bad == 0);
+  if (bad) { if (bad > 0) atomicOr(sflag, bad); return; }
+  const int lane = threadIdx.x & 31;
+  const int leader = __ffs(mask) - 1;
+  int base = 0;
+  if (lane == leader) base = atomicAdd(nent, __popc(mask));
+  base = __shfl_sync(mask, base, leader);
+  const int e = base + __popc(mask & ((1u << lane) - 1u));
+  if (e >= p.ent_cap) { atomicOr(sflag, MODE == 0 ? kFlagOverflow : kFlagSafeOverflow); return; }
+  const int ls = (sx - xs0) * p.G + sy;
   sm.ekey[e] = make_key(z, nz);
-  sm.et[e] = t;
-  sm.elo[e] = lo;
-  sm.enext[e] = atomicExch(&sm.heads[(sx - xs0) * p.G + sy], e);
+  if (MODE == 1) { sm.et[e] = t; sm.elo[e] = lo; }
+  sm.enext[e] = (short)atomicExch(&sm.heads[ls], e);
 }
 
-__global__ void __launch_bounds__(256, 2) k_strip(EngineParams p)
+// Triangle of the current chunk held in registers while its pixels are walked.
+struct TriReg {
+  float ax, ay, az, bx, by, bz, cx, cy, cz, n0, n1, n2;
+  Bary b;
+  float rlo, rvhi, rwhi;   // pre-reject bounds on the sign-adjusted numerators
+  bool dpos;               // denom > 0
+  int t, x0, y0, ylen, xc0;
+};
+
+__device__ __forceinline__ void tri_from_smem(const StripSmem& sm, int ti, TriReg& r)
+{
+  const float4 a4 = sm.q0[ti], b4 = sm.q1[ti], c4 = sm.q2[ti];
+  const int4 tm = sm.tm[ti];
+  r.ax = a4.x; r.ay = a4.y; r.az = a4.z; r.n0 = a4.w;
+  r.bx = b4.x; r.by = b4.y; r.bz = b4.z; r.n1 = b4.w;
+  r.cx = c4.x; r.cy = c4.y; r.cz = c4.z; r.n2 = c4.w;
+  TriGeo g;
+  g.ax = r.ax; g.ay = r.ay; g.bx = r.bx; g.by = r.by; g.cx = r.cx; g.cy = r.cy;
+  bary_setup(g, r.b);
+  const float ad = r.b.denom >= 0.0f ? r.b.denom : -r.b.denom;
+  r.dpos = r.b.denom > 0.0f;
+  r.rlo = __fmul_rn(-0.002f, ad);
+  r.rvhi = __fmul_rn(1.002f, ad);
+  r.rwhi = __fmul_rn(1.004f, ad);
+  r.t = tm.x; r.x0 = tm.y; r.y0 = tm.z; r.ylen = tm.w; r.xc0 = sm.tm2[ti].x;
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(256, MODE == 0 ? 3 : 1) k_strip(EngineParams p)
 {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ int nent, sflag, wtot[32];
@@ -637,69 +767,85 @@ __global__ void __launch_bounds__(256, 2) k_strip(EngineParams p)
   const int C = p.ent_cap;
   const int xs0 = s * p.H, xs1 = min(xs0 + p.H, p.G);
   const int HGs = (xs1 - xs0) * p.G;   // the last strip may be narrower than H
+  const int nwords = (HG + 31) >> 5;
 
-  // shared-memory carve-up (sizes mirrored by strip_smem_bytes on the host)
+  // shared-memory carve-up (strip_smem_layout gives the total)
   StripSmem sm;
   unsigned char* q = smem;
-  sm.heads = (int*)q; q += ((sizeof(int) * HG + 15) / 16) * 16;   // keep the float4 arrays 16-byte aligned
-  sm.ekey = (unsigned*)q; q += sizeof(unsigned) * C;
-  sm.et = (unsigned*)q; q += sizeof(unsigned) * C;
-  sm.elo = (unsigned*)q; q += sizeof(unsigned) * C;
-  sm.enext = (int*)q; q += sizeof(int) * C;
-  sm.emark = (uint8_t*)q; q += ((C + 15) / 16) * 16;
+  sm.heads = (int*)q; q += round16(sizeof(int) * HG);
+  sm.occ = (unsigned*)q; q += round16(sizeof(unsigned) * nwords);
+  sm.ekey = (unsigned*)q; q += round16(sizeof(unsigned) * C);
+  sm.enext = (short*)q; q += round16(sizeof(short) * C);
+  sm.et = sm.elo = nullptr; sm.emark = nullptr;
+  if (MODE == 1) {
+    sm.et = (unsigned*)q; q += round16(sizeof(unsigned) * C);
+    sm.elo = (unsigned*)q; q += round16(sizeof(unsigned) * C);
+    sm.emark = (uint8_t*)q; q += round16((size_t)C);
+  }
   unsigned char* chunk = q;
   sm.q0 = (float4*)q; q += sizeof(float4) * kChunk;
   sm.q1 = (float4*)q; q += sizeof(float4) * kChunk;
   sm.q2 = (float4*)q; q += sizeof(float4) * kChunk;
   sm.q3 = (float4*)q; q += sizeof(float4) * kChunk;
-  sm.q4 = (float4*)q; q += sizeof(float4) * kChunk;
   sm.tm = (int4*)q; q += sizeof(int4) * kChunk;
-  sm.tm2 = (int4*)q; q += sizeof(int4) * kChunk;
+  sm.tm2 = (int2*)q; q += sizeof(int2) * kChunk;
   sm.pref = (int*)q; q += sizeof(int) * (kChunk + 4);
   sm.thit = (int*)q; q += sizeof(int) * kChunk;
-  sm.rvo = (int*)chunk;
-  sm.rvss = sm.rvo + HG;
-  sm.rtc = sm.rvss + HG;
-
-  for (int i = threadIdx.x; i < HG; i += blockDim.x) sm.heads[i] = -1;
-  if (threadIdx.x == 0) { nent = 0; sflag = 0; }
-  __syncthreads();
+  sm.olist = (short*)chunk;
 
   const int* off = p.bin_off + (size_t)o * (p.S + 1);
   const int lbeg = off[s];
   const int lend = min(off[s + 1], p.bin_cap);
   const int nlist = max(lend - lbeg, 0);
   const int* list = p.bins + (size_t)o * p.bin_cap + lbeg;
+  uint8_t* bedf = p.bedf + (size_t)o * p.G * p.G + (size_t)xs0 * p.G;
+
+  // bed flags of empty slots; occupied ones are overwritten in phase B
+  if (p.bed_type != kBedNone)
+    for (int i = threadIdx.x; i < HGs; i += blockDim.x) bedf[i] = kBfPoss | kBfLand;
+  if (nlist == 0) return;   // strip sums stay zero (k_reset), fold count zero
+
+  {
+    int4* h4 = (int4*)sm.heads;
+    const int4 m1 = make_int4(-1, -1, -1, -1);
+    for (int i = threadIdx.x; i < (HG + 3) / 4; i += blockDim.x) h4[i] = m1;
+  }
+  if (threadIdx.x == 0) { nent = 0; sflag = 0; }
+  __syncthreads();
+
   const Shift sh = load_shift(p, o);
+  const float half = p.half, vmax = p.vmax;
 
   // ---- phase A: rasterize the strip's triangles into shared memory
   for (int cb = 0; cb < nlist; cb += kChunk) {
     const int i = threadIdx.x;
+    const int nchunk = min(kChunk, nlist - cb);
     int npix = 0;
-    if (cb + i < nlist) {
+    if (i < nchunk) {
       const int entry = list[cb + i];
       const int t = entry & 0x7FFFFFFF;
       const int fb_only = (entry < 0) ? 1 : 0;
       TriGeo g;
-      load_tri(p, o, t, sh, g);
+      float4 raw[3];
+      load_tri(p, o, t, sh, g, raw);
       Bary b;
       bary_setup(g, b);
       int xc0, xc1;
-      if (p.mode == 0) { xc0 = max(g.x0, xs0); xc1 = min(g.x1, xs1 - 1); }
+      if (MODE == 0) { xc0 = max(g.x0, xs0); xc1 = min(g.x1, xs1 - 1); }
       else { xc0 = g.x0; xc1 = g.x1; }
       const int ylen = g.y1 - g.y0 + 1;
       if (!fb_only && b.ok && xc0 <= xc1 && ylen > 0) npix = (xc1 - xc0 + 1) * ylen;
-      // kind: 1 = fallback only, 2 = box inside this strip (local fallback decision)
-      const int single = (p.mode == 1) || (min(max(g.x0, 0) / p.H, p.S - 1) == min(max(g.x1, 0) / p.H, p.S - 1));
+      // kind bit 0: fallback only; bit 1: box inside one strip (local fallback decision)
+      const int single = (MODE == 1) || (min(max(g.x0, 0) / p.H, p.S - 1) == min(max(g.x1, 0) / p.H, p.S - 1));
       sm.q0[i] = make_float4(g.ax, g.ay, g.az, g.n0);
       sm.q1[i] = make_float4(g.bx, g.by, g.bz, g.n1);
       sm.q2[i] = make_float4(g.cx, g.cy, g.cz, g.n2);
-      sm.q3[i] = make_float4(b.d00, b.d01, b.d11, b.denom);
-      sm.q4[i] = make_float4(b.e0x, b.e0y, b.e1x, b.e1y);
+      sm.q3[i] = make_float4(centroid(__fsub_rn(raw[0].x, sh.dx), __fsub_rn(raw[1].x, sh.dx), __fsub_rn(raw[2].x, sh.dx)),
+                             centroid(__fsub_rn(raw[0].y, sh.dy), __fsub_rn(raw[1].y, sh.dy), __fsub_rn(raw[2].y, sh.dy)),
+                             centroid(__fsub_rn(raw[0].z, sh.dz), __fsub_rn(raw[1].z, sh.dz), __fsub_rn(raw[2].z, sh.dz)),
+                             0.f);
       sm.tm[i] = make_int4(t, g.x0, g.y0, ylen);
-      sm.tm2[i] = make_int4(xc0, npix, fb_only | (single << 1), 0);
-    } else {
-      sm.tm2[i] = make_int4(0, 0, 0, 0);
+      sm.tm2[i] = make_int2(xc0, fb_only | (single << 1));
     }
     sm.thit[i] = 0;
     int total;
@@ -707,91 +853,150 @@ __global__ void __launch_bounds__(256, 2) k_strip(EngineParams p)
     sm.pref[i] = start;
     if (i == 0) sm.pref[kChunk] = total;
     __syncthreads();
-    const int nchunk = min(kChunk, nlist - cb);
-    for (int j = threadIdx.x; j < total; j += blockDim.x) {
-      // triangle of work item j: last i with pref[i] <= j
+
+    // each thread walks a contiguous range of (triangle, pixel) items
+    const int per = (total + blockDim.x - 1) / blockDim.x;
+    const int j0 = min(i * per, total), j1 = min(j0 + per, total);
+    if (j0 < j1) {
       int lo = 0, hi = nchunk - 1;
       while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
-        if (sm.pref[mid] <= j) lo = mid; else hi = mid - 1;
+        if (sm.pref[mid] <= j0) lo = mid; else hi = mid - 1;
       }
-      const int ti = lo;
-      const int4 tm = sm.tm[ti];
-      const int4 tm2 = sm.tm2[ti];
-      const int k = j - sm.pref[ti];
-      const int x = tm2.x + k / tm.w;
-      const int y = tm.z + k % tm.w;
-      const float4 a4 = sm.q0[ti], b4 = sm.q1[ti], c4 = sm.q2[ti], d4 = sm.q3[ti], e4 = sm.q4[ti];
-      Bary b;
-      b.e0x = e4.x; b.e0y = e4.y; b.e1x = e4.z; b.e1y = e4.w;
-      b.d00 = d4.x; b.d01 = d4.y; b.d11 = d4.z; b.denom = d4.w; b.ok = true;
-      float u, v, w;
-      if (!bary_test(a4.x, a4.y, b, pix_center(x, p.half), pix_center(y, p.half), p.vmax, u, v, w)) continue;
-      sm.thit[ti] = 1;
-      const float px = bary3(a4.x, b4.x, c4.x, u, v, w);
-      const float py = bary3(a4.y, b4.y, c4.y, u, v, w);
-      const float pz = bary3(a4.z, b4.z, c4.z, u, v, w);
-      const float nzf = bary3(a4.w, b4.w, c4.w, u, v, w);
-      const int sx = __float2int_rz(px), sy = __float2int_rz(py);
-      const unsigned lidx = (unsigned)((x - tm.y) * tm.w + (y - tm.z));
-      emit(p, sm, &nent, &sflag, xs0, xs1, sx, sy, to_i16(pz), to_i16(__fmul_rn(nzf, 1000.0f)),
-           (unsigned)tm.x, lidx * 2u);
-      if (p.twin) {
-        const float pz2 = __fadd_rn(pz, (nzf >= 0.0f) ? -p.shell_off : p.shell_off);
-        emit(p, sm, &nent, &sflag, xs0, xs1, sx, sy, to_i16(pz2), to_i16(__fmul_rn(-nzf, 1000.0f)),
-             (unsigned)tm.x, lidx * 2u + 1u);
+      int ti = lo;
+      TriReg r;
+      tri_from_smem(sm, ti, r);
+      const int k = j0 - sm.pref[ti];
+      int x = r.xc0 + k / r.ylen;
+      int y = r.y0 + k % r.ylen;
+      int yend = r.y0 + r.ylen - 1;
+      int tnext = sm.pref[ti + 1];
+      // Per pixel this is _getBaryCoord (Tomo_types.cpp:86-115) with the
+      // x-only products hoisted per column and the "+ 0*0" terms of _dot left
+      // out (they can only turn -0 into +0, which changes no comparison and no
+      // stored value).  A pixel whose sign-adjusted numerators lie clearly
+      // outside the acceptance box -- by twice the 0.001 margin -- is rejected
+      // before the divisions; every such pixel fails the exact test too.
+      float px = pix_center(x, half);
+      float ex0 = __fmul_rn(__fsub_rn(px, r.ax), r.b.e0x);
+      float ex1 = __fmul_rn(__fsub_rn(px, r.ax), r.b.e1x);
+      bool hit_any = false;
+      for (int j = j0; j < j1; j++) {
+        const float e2y = __fsub_rn(pix_center(y, half), r.ay);
+        const float d20 = __fadd_rn(ex0, __fmul_rn(e2y, r.b.e0y));
+        const float d21 = __fadd_rn(ex1, __fmul_rn(e2y, r.b.e1y));
+        const float vn = __fsub_rn(__fmul_rn(r.b.d11, d20), __fmul_rn(r.b.d01, d21));
+        const float wn = __fsub_rn(__fmul_rn(r.b.d00, d21), __fmul_rn(r.b.d01, d20));
+        const float vs = r.dpos ? vn : -vn, ws = r.dpos ? wn : -wn;
+        if (!(vs < r.rlo || vs > r.rvhi || ws < r.rlo || ws > r.rwhi)) {
+          const float v = __fdiv_rn(vn, r.b.denom);
+          const float w = __fdiv_rn(wn, r.b.denom);
+          const float u = __double2float_rn(__dsub_rn(__dsub_rn(1.0, (double)v), (double)w));
+          if ((u >= -0.001f) && (v >= -0.001f) && (v <= vmax) && (__fadd_rn(u, v) <= vmax)) {
+            hit_any = true;
+            const float fx = bary3(r.ax, r.bx, r.cx, u, v, w);
+            const float fy = bary3(r.ay, r.by, r.cy, u, v, w);
+            const float fz = bary3(r.az, r.bz, r.cz, u, v, w);
+            const float fn = bary3(r.n0, r.n1, r.n2, u, v, w);
+            const int sx = __float2int_rz(fx), sy = __float2int_rz(fy);
+            const unsigned lidx = (unsigned)((x - r.x0) * r.ylen + (y - r.y0));
+            emit<MODE>(p, sm, &nent, &sflag, xs0, xs1, sx, sy, to_i16(fz), to_i16(__fmul_rn(fn, 1000.0f)),
+                       (unsigned)r.t, lidx * 2u);
+            if (p.twin) {
+              const float fz2 = __fadd_rn(fz, (fn >= 0.0f) ? -p.shell_off : p.shell_off);
+              emit<MODE>(p, sm, &nent, &sflag, xs0, xs1, sx, sy, to_i16(fz2), to_i16(__fmul_rn(-fn, 1000.0f)),
+                         (unsigned)r.t, lidx * 2u + 1u);
+            }
+          }
+        }
+        // advance to item j + 1
+        if (j + 1 == tnext) {
+          if (hit_any) sm.thit[ti] = 1;
+          hit_any = false;
+          if (j + 1 < j1) {
+            ti++;
+            while (sm.pref[ti + 1] <= j + 1) ti++;   // skip triangles without pixels here
+            tri_from_smem(sm, ti, r);
+            x = r.xc0; y = r.y0; yend = r.y0 + r.ylen - 1;
+            tnext = sm.pref[ti + 1];
+            px = pix_center(x, half);
+            ex0 = __fmul_rn(__fsub_rn(px, r.ax), r.b.e0x);
+            ex1 = __fmul_rn(__fsub_rn(px, r.ax), r.b.e1x);
+          }
+        } else if (++y > yend) {
+          y = r.y0; x++;
+          px = pix_center(x, half);
+          ex0 = __fmul_rn(__fsub_rn(px, r.ax), r.b.e0x);
+          ex1 = __fmul_rn(__fsub_rn(px, r.ax), r.b.e1x);
+        }
       }
+      if (hit_any) sm.thit[ti] = 1;
     }
     __syncthreads();
     // centroid fallback of triangles without any accepted pixel
     if (i < nchunk) {
-      const int kind = sm.tm2[i].z;
+      const int kind = sm.tm2[i].y;
       const bool fb = (kind & 1) || ((kind & 2) && sm.thit[i] == 0);
       if (fb) {
-        const int t = sm.tm[i].x;
-        const int4 ix = p.tri[t];
-        const float4* X = p.xf + (size_t)o * p.nV;
-        const float4 A = X[ix.x], B = X[ix.y], Cc = X[ix.z];
-        const float fx = centroid(__fsub_rn(A.x, sh.dx), __fsub_rn(B.x, sh.dx), __fsub_rn(Cc.x, sh.dx));
-        const float fy = centroid(__fsub_rn(A.y, sh.dy), __fsub_rn(B.y, sh.dy), __fsub_rn(Cc.y, sh.dy));
-        const float fz = centroid(__fsub_rn(A.z, sh.dz), __fsub_rn(B.z, sh.dz), __fsub_rn(Cc.z, sh.dz));
-        const int sx = __float2int_rz(fx), sy = __float2int_rz(fy);
-        emit(p, sm, &nent, &sflag, xs0, xs1, sx, sy, to_i16(fz), to_i16(__fmul_rn(A.w, 1000.0f)), (unsigned)t, 0u);
+        const float4 c3 = sm.q3[i];
+        const float n0 = sm.q0[i].w;
+        const unsigned t = (unsigned)sm.tm[i].x;
+        const int sx = __float2int_rz(c3.x), sy = __float2int_rz(c3.y);
+        emit<MODE>(p, sm, &nent, &sflag, xs0, xs1, sx, sy, to_i16(c3.z), to_i16(__fmul_rn(n0, 1000.0f)), t, 0u);
         if (p.twin) {
-          const float fz2 = __fadd_rn(fz, (A.w >= 0.0f) ? -p.shell_off : p.shell_off);
-          emit(p, sm, &nent, &sflag, xs0, xs1, sx, sy, to_i16(fz2), to_i16(__fmul_rn(-A.w, 1000.0f)), (unsigned)t, 1u);
+          const float fz2 = __fadd_rn(c3.z, (n0 >= 0.0f) ? -p.shell_off : p.shell_off);
+          emit<MODE>(p, sm, &nent, &sflag, xs0, xs1, sx, sy, to_i16(fz2), to_i16(__fmul_rn(-n0, 1000.0f)), t, 1u);
         }
       }
     }
     __syncthreads();
   }
 
-  const bool redo = (p.mode == 0) && (sflag & (kFlagStray | kFlagOverflow));
+  // ---- occupied slots in slot order (bitmap from the list heads -> list)
+  const int wl = (HGs + 31) >> 5;
+  for (int w = threadIdx.x >> 5; w < wl; w += blockDim.x >> 5) {
+    const int ls = (w << 5) + (threadIdx.x & 31);
+    const unsigned bits = __ballot_sync(0xFFFFFFFFu, ls < HGs && sm.heads[ls] >= 0);
+    if ((threadIdx.x & 31) == 0) sm.occ[w] = bits;
+  }
+  __syncthreads();
+  const int wper = (wl + blockDim.x - 1) / blockDim.x;
+  const int w0 = min((int)threadIdx.x * wper, wl), w1 = min(w0 + wper, wl);
+  int ocnt = 0;
+  for (int w = w0; w < w1; w++) ocnt += __popc(sm.occ[w]);
+  int nocc;
+  int obase = block_excl_scan(ocnt, wtot, nocc);
+  for (int w = w0; w < w1; w++) {
+    unsigned bits = sm.occ[w];
+    while (bits) {
+      const int b = __ffs(bits) - 1;
+      bits &= bits - 1;
+      sm.olist[obase++] = (short)((w << 5) + b);
+    }
+  }
+  __syncthreads();
+  const bool redo = (MODE == 0) && (sflag & (kFlagStray | kFlagOverflow));
 
-  // ---- phase B: column stage, contiguous slot range per thread (keeps slot order)
-  const int per = (HGs + blockDim.x - 1) / blockDim.x;
-  const int sb = min(threadIdx.x * per, HGs);
-  const int se = min(sb + per, HGs);
-  long long a_vo = 0, a_vss = 0, a_tc = 0, a_avss = 0, a_atc = 0, a_ent = 0, a_col = 0;
-  int nkeep = 0;
+  // ---- phase B: column stage over the occupied slots, contiguous ranges per
+  // thread; every occupied column's values go to the slot-ordered fold list
+  const int per = (nocc + blockDim.x - 1) / blockDim.x;
+  const int l0 = min((int)threadIdx.x * per, nocc), l1 = min(l0 + per, nocc);
+  long long a_vo = 0, a_vss = 0, a_tc = 0, a_avss = 0, a_atc = 0, a_ent = 0;
   int bx0 = INT_MAX, by0 = INT_MAX, bx1 = -1, by1 = -1;
-  uint8_t* bedf = p.bedf + (size_t)o * p.G * p.G;
   const bool dump = (o == p.dump_slot) && p.dump_cols != nullptr;
+  int4* fv = p.foldv + (size_t)o * p.G * p.G + (size_t)xs0 * p.G;
   if (!redo) {
-    for (int ls = sb; ls < se; ls++) {
+    for (int l = l0; l < l1; l++) {
+      const int ls = sm.olist[l];
       const int gx = xs0 + ls / p.G, gy = ls % p.G;
       const int gslot = gx * p.G + gy;
-      const ColOut c = column(p, sm, sm.heads[ls], dump, gslot);
-      sm.rvo[ls] = c.vo; sm.rvss[ls] = c.vss; sm.rtc[ls] = c.tc;
-      if (c.ndist > 1 && (c.vo | c.vss | c.tc)) nkeep++;
+      const ColOut c = column<MODE>(p, sm, sm.heads[ls], dump, gslot, &sflag);
+      fv[l] = make_int4(c.vo, c.vss, c.tc, ls);
       a_vo += c.vo; a_vss += c.vss; a_tc += c.tc;
       a_avss += (c.vss < 0) ? -c.vss : c.vss; a_atc += (c.tc < 0) ? -c.tc : c.tc;
       a_ent += c.ndist;
-      if (c.ndist > 0) {
-        a_col++;
-        bx0 = min(bx0, gx); bx1 = max(bx1, gx); by0 = min(by0, gy); by1 = max(by1, gy);
-      }
-      if (p.bed_type != kBedNone) bedf[gslot] = bed_flags(p, c);
+      bx0 = min(bx0, gx); bx1 = max(bx1, gx); by0 = min(by0, gy); by1 = max(by1, gy);
+      if (p.bed_type != kBedNone) bedf[ls] = bed_flags(p, c);
       if (dump) {
         int* d = p.dump_cols + (size_t)gslot * 8;
         d[0] = c.ndist; d[1] = c.nfin; d[2] = c.vo; d[3] = c.vss; d[4] = c.tc; d[5] = c.lastz;
@@ -800,21 +1005,11 @@ __global__ void __launch_bounds__(256, 2) k_strip(EngineParams p)
     }
   }
 
-  // ---- phase C: reductions and the slot-ordered fold list
-  int ktot;
-  const int kofs = block_excl_scan(nkeep, wtot, ktot);
-  if (!redo) {
-    int4* fv = p.foldv + (size_t)o * p.G * p.G + (size_t)xs0 * p.G;
-    int w = kofs;
-    for (int ls = sb; ls < se; ls++) {
-      const int vo = sm.rvo[ls], vss = sm.rvss[ls], tc = sm.rtc[ls];
-      if ((vo | vss | tc) != 0) fv[w++] = make_int4(vo, vss, tc, ls);
-    }
-  }
-  long long vals[8] = {a_vo, a_vss, a_tc, a_avss, a_atc, a_ent, a_col, (long long)nkeep};
+  // ---- phase C: reductions
+  long long vals[8] = {a_vo, a_vss, a_tc, a_avss, a_atc, a_ent, (long long)(l1 - l0), 0};
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
-  for (int k = 0; k < 8; k++) {
+  for (int k = 0; k < 7; k++) {
     const long long v = warp_sum(vals[k]);
     if (lane == 0) red[k][wid] = v;
   }
@@ -824,20 +1019,21 @@ __global__ void __launch_bounds__(256, 2) k_strip(EngineParams p)
     bx1 = max(bx1, __shfl_xor_sync(0xFFFFFFFFu, bx1, off2));
     by1 = max(by1, __shfl_xor_sync(0xFFFFFFFFu, by1, off2));
   }
-  if (lane == 0 && bx1 >= 0 && !redo) {
+  __syncthreads();
+  const bool redo2 = (MODE == 0) && (sflag & (kFlagStray | kFlagOverflow));
+  if (lane == 0 && bx1 >= 0 && !redo2) {
     atomicMin(&p.bbox[o * 4 + 0], bx0); atomicMin(&p.bbox[o * 4 + 1], by0);
     atomicMax(&p.bbox[o * 4 + 2], bx1); atomicMax(&p.bbox[o * 4 + 3], by1);
   }
-  __syncthreads();
-  if (threadIdx.x < 8) {
+  if (threadIdx.x < 7) {
     long long v = 0;
     for (int w2 = 0; w2 < (int)(blockDim.x >> 5); w2++) v += red[threadIdx.x][w2];
-    if (!redo && v != 0) atomicAdd((unsigned long long*)&p.acc[(size_t)o * kAccLanes + threadIdx.x], (unsigned long long)v);
+    if (!redo2 && v != 0) atomicAdd((unsigned long long*)&p.acc[(size_t)o * kAccLanes + threadIdx.x], (unsigned long long)v);
     // strip sums for the fold: |column value| <= 2 * grid, so a strip sum fits in int32
-    if (!redo && threadIdx.x < 5) p.foldmeta[((size_t)o * p.S + s) * 8 + threadIdx.x] = (int)v;
+    if (!redo2 && threadIdx.x < 5) p.foldmeta[((size_t)o * p.S + s) * 8 + threadIdx.x] = (int)v;
   }
   if (threadIdx.x == 0) {
-    if (!redo) p.foldcnt[(size_t)o * p.S + s] = ktot;
+    if (!redo2) p.foldcnt[(size_t)o * p.S + s] = nocc;
     if (sflag) atomicOr(&p.flags[o], sflag);
   }
 }
@@ -920,7 +1116,6 @@ __global__ void __launch_bounds__(128) k_fold(EngineParams p)
 {
   __shared__ int4 stage[kFoldChunk];
   __shared__ int s_start;
-  __shared__ long long s_pre[3];
   __shared__ float s_f[3];
   const int o = blockIdx.x;
   if (o >= p.Bo) return;
@@ -949,7 +1144,7 @@ __global__ void __launch_bounds__(128) k_fold(EngineParams p)
       for (int c = 0; c < 3; c++) pre[c] += sv[c];
     }
     s_start = start;
-    for (int c = 0; c < 3; c++) { s_pre[c] = pre[c]; s_f[c] = (float)pre[c]; }
+    for (int c = 0; c < 3; c++) s_f[c] = (float)pre[c];
   }
   __syncthreads();
   const int start = s_start;
@@ -983,21 +1178,16 @@ __global__ void __launch_bounds__(128) k_fold(EngineParams p)
 
 namespace tomo {
 
-size_t strip_smem_bytes(int H, int G, int ent_cap)
+size_t strip_smem_bytes(int mode, int H, int G, int ent_cap)
 {
-  const size_t HG = (size_t)H * G;
-  size_t b = ((sizeof(int) * HG + 15) / 16) * 16;      // heads, padded to 16 bytes
-  b += 4 * sizeof(unsigned) * (size_t)ent_cap;          // key, t, lo, next
-  b += (((size_t)ent_cap + 15) / 16) * 16;              // marks
-  const size_t chunk = 5 * sizeof(float4) * kChunk + 2 * sizeof(int4) * kChunk + sizeof(int) * (2 * kChunk + 4);
-  const size_t results = 3 * sizeof(int) * HG;
-  b += (chunk > results) ? chunk : results;
-  return b;
+  return strip_smem_layout(mode, H, G, ent_cap);
 }
 
-cudaError_t configure_kernels(size_t strip_smem)
+cudaError_t configure_kernels(size_t normal_smem, size_t safe_smem)
 {
-  return cudaFuncSetAttribute(k_strip, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)strip_smem);
+  cudaError_t e = cudaFuncSetAttribute(k_strip<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)normal_smem);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_strip<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)safe_smem);
 }
 
 // Launch bookkeeping: every launch is counted; with timing on, a pair of
@@ -1051,7 +1241,9 @@ cudaError_t launch_bin_count(const EngineParams& p, cudaStream_t main, LaunchLog
 cudaError_t launch_after_count(const EngineParams& p, cudaStream_t main, size_t strip_smem, LaunchLog* L)
 {
   TOMO_LAUNCH(kKFill, main, (k_bin_fill<<<tri_grid(p), 256, 2 * sizeof(int) * p.S, main>>>(p)));
-  TOMO_LAUNCH(kKStrip, main, (k_strip<<<dim3(p.S, p.Bo), 256, strip_smem, main>>>(p)));
+  const int kind = p.variant == 0 ? kKStrip : kKStripRedo;
+  if (p.mode == 0) TOMO_LAUNCH(kind, main, (k_strip<0><<<dim3(p.S, p.Bo), 256, strip_smem, main>>>(p)));
+  else TOMO_LAUNCH(kind, main, (k_strip<1><<<dim3(p.S, p.Bo), 256, strip_smem, main>>>(p)));
   TOMO_LAUNCH(kKBed, main, (k_bed<<<dim3(8, p.Bo), 256, 0, main>>>(p)));
   return cudaGetLastError();
 }

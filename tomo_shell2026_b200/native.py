@@ -22,7 +22,7 @@ _i16p = ct.POINTER(ct.c_int16)
 _u32p = ct.POINTER(ct.c_uint32)
 _i64p = ct.POINTER(ct.c_int64)
 
-TOMO_OPT_BATCH, TOMO_OPT_STRIP_H, TOMO_OPT_FORCE_SAFE = 1, 2, 3
+TOMO_OPT_BATCH, TOMO_OPT_STRIP_H, TOMO_OPT_FORCE_SAFE, TOMO_OPT_NORMAL_SMEM = 1, 2, 3, 4
 
 # (name, restype, argtypes) for every export of include/tomo_b200.h
 EXPORTS = [
@@ -111,7 +111,8 @@ def vol_to_mass(f32info, i32info, vm22) -> np.ndarray:
     return vm
 
 
-KERNEL_KINDS = ("k_reset", "k_rotate", "k_bin_count", "k_bin_scan", "k_bin_fill", "k_strip", "k_bed", "k_fold")
+KERNEL_KINDS = ("k_reset", "k_rotate", "k_bin_count", "k_bin_scan", "k_bin_fill", "k_strip", "k_bed", "k_fold",
+                "k_strip_redo")
 
 
 def profile(enable: bool, reset: bool = True) -> None:
@@ -137,7 +138,7 @@ def stats() -> dict:
     out = np.zeros(8, np.int64)
     lib().tomoGetStats(_p(out, _i64p), 8)
     return dict(grid=int(out[0]), strip_h=int(out[1]), strips=int(out[2]), ent_cap=int(out[3]),
-                safe_reruns=int(out[4]), n_ypr=int(out[5]), batch=int(out[6]))
+                overflow_reruns=int(out[4]), n_ypr=int(out[5]), batch=int(out[6]), safe_reruns=int(out[7]))
 
 
 @dataclass
