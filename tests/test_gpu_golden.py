@@ -1,0 +1,45 @@
+"""The CUDA path, through TomoSh_CUDA, against the golden fixtures made by
+the reference INT3 engine.  Bit-exact on every output."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from tests.test_golden import GOLDEN, bits, load_case
+from tomo_shell2026_b200 import native
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=[p.stem for p in GOLDEN])
+def test_cuda_matches_golden(path):
+    d, mesh, opts = load_case(path)
+    r = native.sweep(mesh, d["ypr"], opts)
+    assert np.array_equal(bits(r.Mo), bits(d["Mo"])), "Mo differs"
+    assert np.array_equal(bits(r.Mss), bits(d["Mss"])), "Mss differs"
+    assert np.array_equal(bits(r.Vtc), bits(d["Vtc"])), "Vtc differs"
+    assert np.array_equal(bits(r.VoF), bits(d["VoF"])), "VoF differs"
+    assert np.array_equal(bits(r.VssF), bits(d["VssF"])), "VssF differs"
+    assert np.array_equal(r.Vo64, d["Vo64"]) and np.array_equal(r.Vss64, d["Vss64"]) and np.array_equal(r.Vtc64, d["Vtc64"])
+    assert r.optID == int(d["optID"])
+    assert np.array_equal(bits(r.mat4x4.ravel()), bits(d["mat16"])), "mat4x4 of the best orientation differs"
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=[p.stem for p in GOLDEN])
+def test_cuda_columns_match_golden(path):
+    d, mesh, opts = load_case(path)
+    sess = native.Session(mesh, d["ypr"], opts)
+    assert sess.grid() == 256
+    c = sess.columns(int(d["col_index"]))
+    cols = c["cols"]
+    slots = d["col_slots"]
+    nvox = np.zeros(256 * 256, np.int64)
+    nvox[slots] = d["col_nvox"]
+    assert np.array_equal(cols[:, 0], nvox), "distinct pixels per column differ"
+    paired = d["col_nvox"] > 1
+    assert np.array_equal(cols[slots, 2], d["col_vo"]) and np.array_equal(cols[slots, 3], d["col_vss"])
+    for s, n, nv, o in zip(slots[paired], d["col_nfin"][paired], d["col_nvox"][paired], d["col_off"][:-1][paired]):
+        rows = d["col_rows"][o:o + nv]
+        keys = ((rows[:, 1].astype(np.int64) + 32768) << 16) | (rows[:, 2].astype(np.int64) + 32768)
+        assert np.array_equal(c["keys"][s, :nv], keys), f"column {s} order differs"
+        assert np.array_equal(c["types"][s, :nv], rows[:, 0] & ~32), f"column {s} types differ"
