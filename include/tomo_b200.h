@@ -45,6 +45,11 @@ extern "C" {
 int TomoSh_CUDA(float* f32info, int* i32info, float* YPR, int* tri, float* vtx, float* vtx_nrm, float* tri_nrm,
                 int* chull_tri, float* chull_vtx, float* chull_trinrm);
 
+/* Same call under the reference's CPU-engine name (Tomo_Shell2026.h:33,
+ * Tomo_Shell2026.cpp:296-299): the reference INT3 results, computed on the GPU. */
+int TomoSh_INT3(float* f32info, int* i32info, float* YPR, int* tri, float* vtx, float* vtx_nrm, float* tri_nrm,
+                int* chull_tri, float* chull_vtx, float* chull_trinrm);
+
 /* getMss / getMo / getVtc: [nYPR] float32 (Tomo_Shell2026.h:21-23). */
 float* getMss(void);
 float* getMo(void);
@@ -85,6 +90,7 @@ void tomoVolToMass(const float* f32info, const int* i32info, float* vm22);
 #define TOMO_OPT_STRIP_H 2      /* force strip height 1, 2, 4 or 8 (0 = automatic) */
 #define TOMO_OPT_FORCE_SAFE 3   /* 1 = evaluate every orientation in safe mode */
 #define TOMO_OPT_NORMAL_SMEM 4  /* shared-memory bytes of a normal strip CTA (0 = 72 KB, three per SM) */
+#define TOMO_OPT_EXPORT 5       /* 0 = skip the best orientation's pixel export (default 1) */
 int tomoSetOption(int key, int value);
 
 /* out[0..7] = grid edge, strip height, strips, entry capacity, orientations re-run

@@ -124,6 +124,9 @@ class RefEngine:
         L.ref_int3_columns.restype = ct.c_int
         L.ref_int3_columns.argtypes = [_f32p, _i32p, _f32p, _i32p, _f32p, _f32p, _f32p, _i32p, _f32p, _f32p,
                                        ct.c_int, ct.c_int, _i32p, _i16p, _i32p, _i16p, _i32p, _i32p, _f32p, _f32p]
+        L.ref_int3_pixels.restype = ct.c_int
+        L.ref_int3_pixels.argtypes = [_f32p, _i32p, _f32p, _i32p, _f32p, _f32p, _f32p, _i32p, _f32p, _f32p,
+                                      ct.c_int, ct.c_int, _i32p, _i16p, ct.c_int, _f32p, _f32p]
         L.ref_int3_rotation.restype = ct.c_float
         L.ref_int3_rotation.argtypes = [ct.c_float, ct.c_float, ct.c_float, _f32p]
 
@@ -131,6 +134,23 @@ class RefEngine:
         out = np.zeros(16, np.float32)
         self.lib.ref_int3_rotation(yaw, pitch, roll, _p(out, _f32p))
         return out.reshape(4, 4)[:3, :3].copy()
+
+    def pixels(self, mesh, ypr, opts, index: int, grid: int = 256, max_pixels: int = 4_000_000) -> dict:
+        """Render pixels, vm_info and mat4x4 of one orientation, as exported
+        by the reference after its best-orientation re-run."""
+        f32, i32, ypr, tri, vtx, vn, tn, htri, hv, hn = _inputs(mesh, ypr, opts)
+        counts = np.zeros(11, np.int32)
+        buf = np.zeros((max_pixels, 6), np.int16)
+        vm = np.zeros(22, np.float32)
+        mat = np.zeros(16, np.float32)
+        total = self.lib.ref_int3_pixels(
+            _p(f32, _f32p), _p(i32, _i32p), _p(ypr, _f32p), _p(tri, _i32p), _p(vtx, _f32p), _p(vn, _f32p),
+            _p(tn, _f32p), _p(htri, _i32p), _p(hv, _f32p), _p(hn, _f32p), index, grid,
+            _p(counts, _i32p), _p(buf, _i16p), max_pixels, _p(vm, _f32p), _p(mat, _f32p))
+        if total > max_pixels:
+            raise RuntimeError("pixel buffer too small")
+        off = np.concatenate([[0], np.cumsum(counts)])
+        return dict(pixels=[buf[off[k]:off[k + 1]].copy() for k in range(11)], vm22=vm, mat16=mat)
 
     def sweep(self, mesh, ypr, opts, grid: int = 256, threads: int | None = None, exact: bool = True) -> dict:
         args = _inputs(mesh, ypr, opts)

@@ -235,9 +235,48 @@ int ref_int3_columns(const float* f32info, const int* i32info, const float* ypr,
   return 0;
 }
 
-// The float the engine uses for the shadow threshold, read back from the
-// reference translation unit's own expression (cpu_src/STomoSh_INT3.cpp:756).
-// Exposed so the restatement can be pinned to the same overload of ::sin.
+// The export tail of _TomoSh_Function_Call (Tomo_Shell2026.cpp:218-244) for
+// one orientation: thread_func on it, then slotsToPxls for every pixel type
+// with GetSSPixels in the eptSS entry, mat4x4 and vm_info.  counts[11] gets
+// the pixel count per type; pixels receives the concatenated n x 6 int16
+// records (type 0 first) up to max_pixels; returns the total count.
+int ref_int3_pixels(const float* f32info, const int* i32info, const float* ypr,
+                    const int* tri, const float* vtx, const float* vnrm, const float* tnrm,
+                    const int* htri, const float* hvtx, const float* htnrm,
+                    int ypr_index, int grid, int* counts, short* pixels, int max_pixels,
+                    float* volmass22, float* mat16)
+{
+  S3DPrinterInfo info(const_cast<float*>(f32info), const_cast<int*>(i32info), const_cast<int*>(tri),
+                      const_cast<float*>(vtx), const_cast<float*>(vnrm), const_cast<float*>(tnrm),
+                      const_cast<int*>(htri), const_cast<float*>(hvtx), const_cast<float*>(htnrm), 0, 0, 0);
+  STomoSh_INT3* nv = new STomoSh_INT3[1];
+  prepare(nv, 1, info, grid);
+  S3DPrinterInfo& pi = nv->printer_info;
+  pi.yaw = ypr[ypr_index * 3 + 0];
+  pi.pitch = ypr[ypr_index * 3 + 1];
+  pi.roll = ypr[ypr_index * 3 + 2];
+  nv->Rotate();
+  nv->Pixelize();
+  nv->Pairing();
+  nv->GenerateBed();
+  nv->Calculate();
+  int total = 0;
+  for (int i = 0; i < g_nPixelType; i++) {
+    TPVector px = (i == static_cast<int>(enumPixelType::eptSS)) ? nv->GetSSPixels(pi.bUseExplicitSS)
+                                                                : nv->slotsToPxls(enumPixelType(i));
+    counts[i] = static_cast<int>(px.size());
+    for (auto& q : px) {
+      if (total < max_pixels) q.DumpTo(pixels + static_cast<size_t>(total) * 6);
+      total++;
+    }
+  }
+  if (volmass22 != nullptr) std::memcpy(volmass22, nv->vm_info.dData, sizeof(float) * 22);
+  if (mat16 != nullptr) std::memcpy(mat16, nv->mat4x4.fData, sizeof(float) * 16);
+  delete[] nv;
+  return total;
+}
+
+// SMatrix4f(yaw, pitch, roll) as built by the reference (cpu_src/SMatrix4f.cpp:8-12,213-240).
 float ref_int3_rotation(float yaw, float pitch, float roll, float* out16)
 {
   SMatrix4f m(yaw, pitch, roll);

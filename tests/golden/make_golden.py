@@ -74,8 +74,11 @@ def main():
         occ = np.nonzero(d["n_fin"])[0].astype(np.int32)
         rows = [d["fin_tzn"][s, : d["n_fin"][s]] for s in occ]
         off = np.concatenate([[0], np.cumsum([r.shape[0] for r in rows])]).astype(np.int32)
+        ex = ref.pixels(mesh, ypr, opts, idx, grid=256)
+        pcount = np.array([px.shape[0] for px in ex["pixels"]], np.int32)
         np.savez_compressed(
             OUT / f"{name}.npz",
+            pix_count=pcount, pix_data=np.concatenate(ex["pixels"], 0).astype(np.int16), pix_vm22=ex["vm22"],
             f32info=f32, i32info=i32, ypr=ypr, vertices=mesh.vertices, faces=mesh.faces,
             vertex_normals=mesh.vertex_normals, face_normals=mesh.face_normals, area=np.float64(mesh.area),
             Mo=out["Mo"], Mss=out["Mss"], Vtc=out["Vtc"], VoF=out["VoF"], VssF=out["VssF"],

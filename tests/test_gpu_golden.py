@@ -43,3 +43,18 @@ def test_cuda_columns_match_golden(path):
         keys = ((rows[:, 1].astype(np.int64) + 32768) << 16) | (rows[:, 2].astype(np.int64) + 32768)
         assert np.array_equal(c["keys"][s, :nv], keys), f"column {s} order differs"
         assert np.array_equal(c["types"][s, :nv], rows[:, 0] & ~32), f"column {s} types differ"
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=[p.stem for p in GOLDEN])
+def test_cuda_export_matches_golden(path):
+    """Best-orientation render data (getnData2i/getpData2i per pixel type, the
+    SS pixels of GetSSPixels in type 4) and getVolMassInfo, as the reference
+    exports them after re-running optID (Tomo_Shell2026.cpp:218-244)."""
+    d, mesh, opts = load_case(path)
+    r = native.sweep(mesh, d["ypr"], opts)
+    off = np.concatenate([[0], np.cumsum(d["pix_count"])])
+    for k in range(11):
+        want = d["pix_data"][off[k]:off[k + 1]]
+        assert r.pixels[k].shape == want.shape, f"pixel type {k}: {r.pixels[k].shape[0]} vs {want.shape[0]}"
+        assert np.array_equal(r.pixels[k], want), f"pixel type {k} differs"
+    assert np.array_equal(bits(r.volmass), bits(d["pix_vm22"])), "vm_info differs"

@@ -218,6 +218,7 @@ struct Engine {
   int force_h = 0;        // test hook: strip height override
   int force_safe = 0;     // test hook: run every orientation in safe mode
   int normal_smem = 0;    // shared-memory budget of a normal strip CTA (0 = 72 KB)
+  int export_pixels = 1;  // rebuild the best orientation's pixels and vm_info (TomoSh_CUDA tail)
   float cx = 0, cy = 0, cz = 0;
   std::vector<float> h_rot;
   std::vector<long long> vo64, vss64, vtc64, entries, columns;
@@ -600,12 +601,14 @@ struct Engine {
   }
 
   // One orientation with the dense per-column dump enabled (parity tests).
-  int dump(int id, int mode, int* cols8, unsigned* keys64, short* types64)
+  int dump(int id, int c, int* cols8, unsigned* keys64, short* types64)
   {
     if (id < 0 || id >= nYPR) return set_error(TOMO_ERR_ARG, "orientation index out of range");
     if (P.n_tri == 0) return set_error(TOMO_ERR_ARG, "empty mesh");
-    choose_strips(mode);
-    const size_t smem = cfg[mode].smem;
+    if (c < 0 || c > 3) return set_error(TOMO_ERR_ARG, "bad strip configuration");
+    choose_strips(c);
+    const int mode = cfg[c].mode;
+    const size_t smem = cfg[c].smem;
     TOMO_TRY(configure());
     TOMO_TRY(reserve_outputs());
     const size_t GG = (size_t)G * G;
@@ -706,6 +709,132 @@ void host_mat4x4(const Engine& E, const float* vtx, int nV, int id, float* m16)
   m16[7] = -dy + R[3] * m + R[4] * n + R[5] * o;
   m16[11] = -dz + R[6] * m + R[7] * n + R[8] * o;
 }
+// Final slot rows of one orientation rebuilt on the host from its column
+// dump: kept pixels in column order with their paired types, the floor
+// sentinels (STomoSh_INT3.cpp:790-810) and the bed pixels (GenerateBed,
+// :1375-1443) -- the reference's slot buffer after thread_func.  From them:
+// the render pixels of slotsToPxls (:1103-1135) and GetSSPixels
+// (:1257-1318, brief branch) and the vm_info of Calculate (:1211-1255).
+struct SlotRow { short type, z, nz; };
+
+bool host_bed_candidate(const Engine& E, const std::vector<uint8_t>& bf, int X, int Y)
+{
+  const int G = E.G, r = (int)E.P.bed_outer;
+  const int xa = std::max(X - r, 0), xb = std::min(X + r, G), ya = std::max(Y - r, 0), yb = std::min(Y + r, G);
+  const int qid = X * G + Y;
+  float md = 1e5f;
+  for (int sx = xa; sx < xb; sx++)
+    for (int sy = ya; sy < yb; sy++) {
+      const int sid = sx * G + sy;
+      const uint8_t f = bf[sid];
+      if (!(f & kBfTouch)) continue;
+      if ((f & kBfSelfR) && sid < qid) continue;
+      const float dx = (float)X - (float)sx, dy = (float)Y - (float)sy;
+      const float dist = sqrtf(dx * dx + dy * dy);
+      md = (md < dist) ? md : dist;
+    }
+  if (md > E.P.bed_outer) return false;
+  if (E.P.bed_type == kBedBrim || E.P.bed_type == kBedRaft) return true;
+  if (E.P.bed_type == kBedSkirt && md > E.P.bed_inner) return true;
+  return false;
+}
+
+int export_best(Engine& E, int id, std::vector<short>* pix, int* npix, float* vm)
+{
+  const int G = E.G;
+  const size_t GG = (size_t)G * G;
+  std::vector<int> cols(GG * 8);
+  std::vector<unsigned> keys(GG * 64);
+  std::vector<short> types(GG * 64);
+  int fl = -1;
+  for (int c : {0, 1, 3}) {
+    fl = E.dump(id, c, cols.data(), keys.data(), types.data());
+    if (fl < 0) return fl;
+    if (!(fl & (kFlagStray | kFlagOverflow | kFlagBinCap | kFlagSafeOverflow))) break;
+  }
+  if (fl & (kFlagStray | kFlagOverflow | kFlagBinCap | kFlagSafeOverflow | kFlagGrid))
+    return set_error(TOMO_ERR_CAPACITY, "best orientation could not be exported");
+  std::vector<std::vector<SlotRow>> rows(GG);
+  std::vector<uint8_t> bf(GG, (uint8_t)(kBfPoss | kBfLand));
+  int minX = G, minY = G, maxX = -1, maxY = -1;
+  for (size_t sl = 0; sl < GG; sl++) {
+    const int* c = &cols[sl * 8];
+    const int nd = c[0], nfin = c[1];
+    if (nd == 0) continue;
+    const int x = (int)(sl / G), y = (int)(sl % G);
+    minX = std::min(minX, x); maxX = std::max(maxX, x); minY = std::min(minY, y); maxY = std::max(maxY, y);
+    auto& r = rows[sl];
+    for (int i = 0; i < nd && i < 64; i++) {
+      const unsigned k = keys[sl * 64 + i];
+      r.push_back({nd > 1 ? types[sl * 64 + i] : (short)0, (short)((int)(k >> 16) - 32768), (short)((int)(k & 0xFFFFu) - 32768)});
+    }
+    const int extra = nfin - nd;
+    if (extra == 2) { r.push_back({(short)kSSA, 0, 0}); r.push_back({(short)kNVA, 0, 0}); }
+    else if (extra == 1) r.push_back({(short)c[6], 0, 0});
+    bf[sl] = (uint8_t)c[7];
+  }
+  // bed pixels, in the reference's scan order
+  if (E.P.bed_type != kBedNone && maxX >= 0 && (int)E.P.bed_outer > 0) {
+    const int m = (int)E.P.bed_outer + 1;
+    const int bx0 = std::max(minX - m, 0), bx1 = std::min(maxX + m + 1, G);
+    const int by0 = std::max(minY - m, 0), by1 = std::min(maxY + m + 1, G);
+    for (int X = bx0; X < bx1; X++)
+      for (int Y = by0; Y < by1; Y++) {
+        const size_t sl = (size_t)X * G + Y;
+        const uint8_t f = bf[sl];
+        if (!((f & kBfPoss) && (f & kBfLand)) || !host_bed_candidate(E, bf, X, Y)) continue;
+        auto& r = rows[sl];
+        bool merged = false;
+        for (auto& q : r)
+          if (q.z == 1 && q.nz == 0) { q.type |= (short)kBed; merged = true; break; }
+        if (!merged) r.push_back({(short)kBed, 1, 0});
+      }
+  }
+  // render pixels per type (slotsToPxls) and the support pixels (GetSSPixels)
+  for (int k = 0; k < 11; k++) pix[k].clear();
+  for (size_t sl = 0; sl < GG; sl++) {
+    if (rows[sl].empty()) continue;
+    const short x = (short)(sl / G), y = (short)(sl % G);
+    for (const auto& q : rows[sl])
+      for (int k = 0; k < 11; k++)
+        if (k != 4 && (q.type & (1 << k))) {
+          const short px[6] = {x, y, q.z, 0, 0, q.nz};
+          pix[k].insert(pix[k].end(), px, px + 6);
+        }
+    int ss0 = -1, ss1 = -1;
+    for (const auto& q : rows[sl]) {
+      if (q.type & kSSB) ss0 = q.z;
+      if (q.type & kSSA) ss1 = q.z;
+      if (ss0 > -1 && ss1 > -1) {
+        for (int zz = ss0; zz >= ss1; zz--) {
+          const short px[6] = {x, y, (short)zz, 0, 0, 0};
+          pix[4].insert(pix[4].end(), px, px + 6);
+        }
+        ss0 = ss1 = -1;
+      }
+    }
+  }
+  for (int k = 0; k < 11; k++) npix[k] = (int)(pix[k].size() / 6);
+  // Calculate: float folds over the occupied slots in ascending order
+  float va = 0.f, vb = 0.f, vnv = 0.f, vtc = 0.f, vbed = 0.f;
+  for (size_t sl = 0; sl < GG; sl++) {
+    if (rows[sl].empty()) continue;
+    int sa = 0, sb = 0, snvb = 0, snva = 0, stc = 0, sbed = 0;
+    for (const auto& q : rows[sl]) {
+      if (q.type & kAl) sa += q.z;
+      if (q.type & kBe) sb += q.z;
+      if (q.type & kNVB) snvb += q.z;
+      if (q.type & kNVA) snva += q.z;
+      if (q.type & kTC) stc += q.z;
+      if (q.type & kBed) sbed += q.z;
+    }
+    va += (float)sa; vb += (float)sb; vnv += (float)(snvb - snva); vtc += (float)stc;
+    vbed += (float)sbed * E.P.bed_thickness;
+  }
+  vm[0] = va; vm[1] = vb; vm[2] = vtc; vm[3] = vnv; vm[11] = vbed;
+  return 0;
+}
+
 }  // namespace
 
 }  // namespace tomo
@@ -738,13 +867,27 @@ int TomoSh_CUDA(float* f32info, int* i32info, float* YPR, int* tri, float* vtx, 
   g_Vo64 = E.vo64; g_Vss64 = E.vss64; g_Vtc64 = E.vtc64;
   const int opt = first_optimal(n, g_Mss.data());
   std::memset(g_volmass, 0, sizeof(g_volmass));
+  for (int k = 0; k < 11; k++) { g_pix[k].clear(); g_npix[k] = 0; }
   if (n > 0) {
-    g_volmass[8] = E.vof[opt]; g_volmass[4] = E.vssf[opt]; g_volmass[2] = E.vtcf[opt];
+    if (E.P.n_tri > 0 && E.export_pixels) {
+      rc = export_best(E, opt, g_pix, g_npix, g_volmass);
+      if (rc) return rc;
+    } else {
+      g_volmass[2] = E.vtcf[opt];
+    }
+    g_volmass[8] = E.vof[opt]; g_volmass[4] = E.vssf[opt];
     vol_to_mass(E.P, g_volmass);
     host_mat4x4(E, vtx, E.P.n_vtx, opt, g_mat4x4);
   }
-  for (int k = 0; k < 11; k++) { g_pix[k].clear(); g_npix[k] = 0; }
   return opt;
+}
+
+// The reference exports the CPU engine under this name (Tomo_Shell2026.cpp:257-260);
+// here it is the same B200 computation, whose results are the INT3 results.
+int TomoSh_INT3(float* f32info, int* i32info, float* YPR, int* tri, float* vtx, float* vtx_nrm, float* tri_nrm,
+                int* chull_tri, float* chull_vtx, float* chull_trinrm)
+{
+  return TomoSh_CUDA(f32info, i32info, YPR, tri, vtx, vtx_nrm, tri_nrm, chull_tri, chull_vtx, chull_trinrm);
 }
 
 float* getMss(void) { return g_Mss.empty() ? nullptr : g_Mss.data(); }
@@ -793,6 +936,7 @@ int tomoSetOption(int key, int value)
     case TOMO_OPT_STRIP_H: if (value < 0 || value > 8) return TOMO_ERR_ARG; E.force_h = value; return 0;
     case TOMO_OPT_FORCE_SAFE: E.force_safe = value ? 1 : 0; return 0;
     case TOMO_OPT_NORMAL_SMEM: if (value < 0 || value > 232448) return TOMO_ERR_ARG; E.normal_smem = value; return 0;
+    case TOMO_OPT_EXPORT: E.export_pixels = value ? 1 : 0; return 0;
     default: return TOMO_ERR_ARG;
   }
 }

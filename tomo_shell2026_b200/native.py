@@ -22,11 +22,12 @@ _i16p = ct.POINTER(ct.c_int16)
 _u32p = ct.POINTER(ct.c_uint32)
 _i64p = ct.POINTER(ct.c_int64)
 
-TOMO_OPT_BATCH, TOMO_OPT_STRIP_H, TOMO_OPT_FORCE_SAFE, TOMO_OPT_NORMAL_SMEM = 1, 2, 3, 4
+TOMO_OPT_BATCH, TOMO_OPT_STRIP_H, TOMO_OPT_FORCE_SAFE, TOMO_OPT_NORMAL_SMEM, TOMO_OPT_EXPORT = 1, 2, 3, 4, 5
 
 # (name, restype, argtypes) for every export of include/tomo_b200.h
 EXPORTS = [
     ("TomoSh_CUDA", ct.c_int32, [_f32p, _i32p, _f32p, _i32p, _f32p, _f32p, _f32p, _i32p, _f32p, _f32p]),
+    ("TomoSh_INT3", ct.c_int32, [_f32p, _i32p, _f32p, _i32p, _f32p, _f32p, _f32p, _i32p, _f32p, _f32p]),
     ("getMss", _f32p, []),
     ("getMo", _f32p, []),
     ("getVtc", _f32p, []),
@@ -159,6 +160,18 @@ class SweepResult:
     columns: np.ndarray
     volmass: np.ndarray
     mat4x4: np.ndarray
+    pixels: list  # 11 arrays of (n, 6) int16 records x,y,z,nx,ny,nz, one per pixel type
+
+
+def pixels() -> list:
+    """getnData2i/getpData2i of the last sweep, one (n, 6) int16 array per type."""
+    L = lib()
+    out = []
+    for k in range(11):
+        n = int(L.getnData2i(k))
+        p = L.getpData2i(k)
+        out.append(np.ctypeslib.as_array(p, shape=(n, 6)).copy() if n and p else np.zeros((0, 6), np.int16))
+    return out
 
 
 def _arrays(mesh, ypr):
@@ -194,7 +207,7 @@ def sweep(mesh, ypr, opts) -> SweepResult:
     return SweepResult(opt, get(L.getMo), get(L.getMss), get(L.getVtc), r["Vo64"], r["Vss64"], r["Vtc64"],
                        r["VoF"], r["VssF"], r["VtcF"], r["n_bed"], r["flags"], r["entries"], r["columns"],
                        np.ctypeslib.as_array(L.getVolMassInfo(), shape=(22,)).copy(),
-                       np.ctypeslib.as_array(L.getMat4x4(), shape=(16,)).copy().reshape(4, 4))
+                       np.ctypeslib.as_array(L.getMat4x4(), shape=(16,)).copy().reshape(4, 4), pixels())
 
 
 class Session:
