@@ -131,6 +131,32 @@ int tomoGridSize(void);
  * Returns the orientation's status flags (>= 0) or a negative error. */
 int tomoColumnDump(int ypr_index, int safe_mode, int* cols8, unsigned* keys64, short* types64);
 
+/* Allocation-free form of TomoSh_CUDA for small meshes.  No counterpart in the
+ * reference.  Same inputs as TomoSh_CUDA; Mo, Mss and Vtc are caller-owned
+ * host arrays of nYPR floats that receive what getMo/getMss/getVtc return
+ * after TomoSh_CUDA, and the return value is optID (or a negative error).
+ * The render pixels, vm_info and mat4x4 are not produced.
+ *   - allocates nothing: device scratch is one file-scope 8 MiB __device__
+ *     array per device, host staging is file-scope arrays; no cudaMalloc,
+ *     cudaFree or allocating library routine is called;
+ *   - limits: at most 16384 triangles and 16384 vertices, and a footprint
+ *     within the reference's 256 x 256 slot grid; larger inputs return
+ *     TOMO_ERR_CAPACITY with the limit in tomoGetLastErrorString();
+ *   - the scratch's device address is looked up with cudaGetSymbolAddress the
+ *     first time a device is used (with that device current), so make the first
+ *     call on each device before any stream capture begins;
+ *   - nothing has to start at zero: each batch clears what its kernels
+ *     accumulate into (the bed pixel counts by cudaMemsetAsync, the rest in
+ *     the first kernel);
+ *   - the scratch is shared by every call on a device, so two calls whose
+ *     device work overlapped would race on it; the call holds the library's
+ *     lock and synchronizes `stream` before it returns, so calls from several
+ *     host threads run one after another;
+ *   - work is issued on `stream` (a cudaStream_t; null = the legacy default
+ *     stream), orientations four at a time. */
+int tomoSweepStatic(const float* f32info, const int* i32info, const float* YPR, const int* tri, const float* vtx,
+                    const float* vtx_nrm, float* Mo, float* Mss, float* Vtc, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

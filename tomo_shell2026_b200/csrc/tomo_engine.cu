@@ -1061,3 +1061,298 @@ int tomoFinish(float* Mo, float* Mss, float* Vtc)
 }
 
 }  // extern "C"
+
+// ------------------------------------------------ allocation-free sweep
+//
+// tomoSweepStatic: the orientation search of TomoSh_CUDA for small meshes,
+// with every device buffer carved out of one file-scope __device__ array
+// and every host buffer a file-scope array, so that a call allocates no
+// memory on the device or the host.  The kernels, the strip configurations
+// and the re-run ladder are those of Engine::execute; only the buffers and
+// the batch size (kStaticBatch orientations) differ.
+
+namespace tomo {
+
+constexpr size_t kStaticArenaBytes = size_t(8) << 20;   // 8 MiB of device scratch per device
+constexpr int kStaticMaxTri = 16384;
+constexpr int kStaticMaxVtx = 16384;
+constexpr int kStaticBatch = 4;
+constexpr int kStaticGrid = 256;                        // the reference's slot grid
+constexpr int kStaticMaxDevices = 64;
+
+static __device__ __align__(256) unsigned char g_static_arena[kStaticArenaBytes];
+
+namespace {
+
+constexpr size_t static_round(size_t b) { return (b + 255) & ~size_t(255); }
+
+// Bytes of the arena layout below for nV vertices and nT triangles.
+constexpr size_t static_bytes(size_t nV, size_t nT)
+{
+  const size_t B = kStaticBatch, GG = (size_t)kStaticGrid * kStaticGrid, S = kStaticGrid;  // S bound: 1-column strips
+  return static_round(16 * nV) * 2 + static_round(16 * nT) + static_round(4 * 9 * B) + static_round(4 * B) +
+         static_round(16 * B * nV) + static_round(4 * 4 * B) + static_round(4 * B * nT) +
+         static_round(4 * B * (S + 1)) + static_round(4 * B * S) + static_round(4 * B * (4 * nT + 4096)) +
+         static_round(4 * 4 * B) + static_round(B * GG) + static_round(8 * B * kAccLanes) + static_round(4 * B) +
+         static_round(4 * B * S) + static_round(16 * B * GG) + static_round(4 * B * S * 8) +
+         5 * static_round(8 * B) + 3 * static_round(4 * B) + 2 * static_round(4 * B);
+}
+static_assert(static_bytes(kStaticMaxVtx, kStaticMaxTri) <= kStaticArenaBytes,
+              "the static scratch must hold the largest accepted mesh");
+
+struct StaticLayout {
+  float4 *vpos, *vnrm, *xf;
+  int4* tri;
+  float* rot;
+  int *ori, *bin_off, *bin_cur, *bins, *bbox, *flags, *foldcnt, *foldmeta, *o_nbed, *o_flags;
+  unsigned *minkey, *trange;
+  uint8_t* bedf;
+  long long *acc, *o_vo, *o_vss, *o_vtc, *o_ent, *o_col;
+  int4* foldv;
+  float *o_vof, *o_vssf, *o_vtcf;
+  long long bins_total;   // entries of the bins region
+};
+
+// Same order and sizes as static_bytes().
+StaticLayout static_layout(unsigned char* base, int nV, int nT)
+{
+  const size_t B = kStaticBatch, GG = (size_t)kStaticGrid * kStaticGrid, S = kStaticGrid;
+  size_t off = 0;
+  auto take = [&](size_t bytes) { unsigned char* q = base + off; off += static_round(bytes); return (void*)q; };
+  StaticLayout L;
+  L.vpos = (float4*)take(16 * (size_t)nV);
+  L.vnrm = (float4*)take(16 * (size_t)nV);
+  L.tri = (int4*)take(16 * (size_t)nT);
+  L.rot = (float*)take(4 * 9 * B);
+  L.ori = (int*)take(4 * B);
+  L.xf = (float4*)take(16 * B * nV);
+  L.minkey = (unsigned*)take(4 * 4 * B);
+  L.trange = (unsigned*)take(4 * B * nT);
+  L.bin_off = (int*)take(4 * B * (S + 1));
+  L.bin_cur = (int*)take(4 * B * S);
+  L.bins_total = (long long)B * (4 * (long long)nT + 4096);
+  L.bins = (int*)take(4 * (size_t)L.bins_total);
+  L.bbox = (int*)take(4 * 4 * B);
+  L.bedf = (uint8_t*)take(B * GG);
+  L.acc = (long long*)take(8 * B * kAccLanes);
+  L.flags = (int*)take(4 * B);
+  L.foldcnt = (int*)take(4 * B * S);
+  L.foldv = (int4*)take(16 * B * GG);
+  L.foldmeta = (int*)take(4 * B * S * 8);
+  L.o_vo = (long long*)take(8 * B); L.o_vss = (long long*)take(8 * B); L.o_vtc = (long long*)take(8 * B);
+  L.o_ent = (long long*)take(8 * B); L.o_col = (long long*)take(8 * B);
+  L.o_vof = (float*)take(4 * B); L.o_vssf = (float*)take(4 * B); L.o_vtcf = (float*)take(4 * B);
+  L.o_nbed = (int*)take(4 * B); L.o_flags = (int*)take(4 * B);
+  return L;
+}
+
+// Host staging, file-scope so that a call allocates nothing on the host either.
+float4 g_static_hpos[kStaticMaxVtx], g_static_hnrm[kStaticMaxVtx];
+int4 g_static_htri[kStaticMaxTri];
+float g_static_hrot[kStaticBatch * 9];
+int g_static_hori[kStaticBatch] = {0, 1, 2, 3};
+int g_static_hflags[kStaticBatch], g_static_hnbed[kStaticBatch];
+float g_static_hvof[kStaticBatch], g_static_hvssf[kStaticBatch], g_static_hvtcf[kStaticBatch];
+float g_static_bedfold[kStaticGrid * kStaticGrid + 1];
+void* g_static_addr[kStaticMaxDevices];
+static_assert(kStaticBatch == 4, "g_static_hori lists the batch slots");
+
+// Device address of g_static_arena on the current device, looked up once per
+// device (with that device current).
+int static_arena(void** out)
+{
+  int dev = 0;
+  TOMO_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kStaticMaxDevices) return set_error(TOMO_ERR_CAPACITY, "device ordinal beyond the static table");
+  if (g_static_addr[dev] == nullptr) {
+    void* a = nullptr;
+    TOMO_CUDA(cudaGetSymbolAddress(&a, g_static_arena));
+    g_static_addr[dev] = a;
+  }
+  *out = g_static_addr[dev];
+  return 0;
+}
+
+void static_bind(EngineParams& p, const StaticLayout& L, int nb, int slot, int bin_cap)
+{
+  p.vpos = L.vpos; p.vnrm = L.vnrm; p.tri = L.tri; p.rot = L.rot;
+  p.ori = L.ori + slot; p.Bo = nb;
+  p.xf = L.xf; p.minkey = L.minkey; p.trange = L.trange;
+  p.bin_off = L.bin_off; p.bin_cur = L.bin_cur; p.bins = L.bins; p.bin_cap = bin_cap;
+  p.acc = L.acc; p.flags = L.flags; p.bbox = L.bbox; p.bedf = L.bedf;
+  p.foldcnt = L.foldcnt; p.foldv = L.foldv; p.foldmeta = L.foldmeta;
+  p.out_vo = L.o_vo; p.out_vss = L.o_vss; p.out_vtc = L.o_vtc; p.out_vof = L.o_vof; p.out_vssf = L.o_vssf;
+  p.out_vtcf = L.o_vtcf; p.out_nbed = L.o_nbed; p.out_flags = L.o_flags; p.out_entries = L.o_ent;
+  p.out_columns = L.o_col;
+  p.dump_slot = -1; p.dump_cols = nullptr; p.dump_keys = nullptr; p.dump_types = nullptr;
+}
+
+// One batch slot re-run in strip configuration c (Engine::run_subset for a
+// single orientation); returns the slot's new status flags or an error.
+int static_rerun(Engine& X, const StaticLayout& L, int slot, int c, cudaStream_t st)
+{
+  X.choose_strips(c);
+  const int mode = X.cfg[c].mode;
+  EngineParams p = X.base_params(mode);
+  p.variant = c;
+  const int normal_cap = 4 * X.P.n_tri + 4096;
+  static_bind(p, L, 1, slot, mode == 0 ? normal_cap : INT_MAX);
+  TOMO_CUDA(cudaMemsetAsync(L.o_nbed + slot, 0, sizeof(int), st));
+  if (mode == 0) {
+    TOMO_CUDA(launch_batch(p, st, X.cfg[c].smem, nullptr));
+  } else {
+    TOMO_CUDA(launch_bin_count(p, st, nullptr));
+    int total = 0;
+    TOMO_CUDA(cudaMemcpyAsync(&total, L.bin_off + X.S, sizeof(int), cudaMemcpyDeviceToHost, st));
+    TOMO_CUDA(cudaStreamSynchronize(st));
+    if ((long long)total > L.bins_total)
+      return set_error(TOMO_ERR_CAPACITY, "tomoSweepStatic: safe-mode strip bins exceed the static scratch");
+    p.bin_cap = std::max(total, 1);
+    TOMO_CUDA(launch_after_count(p, st, X.cfg[c].smem, nullptr));
+  }
+  TOMO_CUDA(launch_fold(p, st, nullptr));
+  int fl = 0;
+  TOMO_CUDA(cudaMemcpyAsync(&fl, L.o_flags + slot, sizeof(int), cudaMemcpyDeviceToHost, st));
+  TOMO_CUDA(cudaStreamSynchronize(st));
+  return fl;
+}
+
+}  // namespace
+}  // namespace tomo
+
+extern "C" int tomoSweepStatic(const float* f32info, const int* i32info, const float* YPR, const int* tri,
+                               const float* vtx, const float* vtx_nrm, float* Mo, float* Mss, float* Vtc,
+                               void* stream)
+{
+  std::lock_guard<std::mutex> lock(g_mutex);
+  g_last_error = 0; g_last_error_str.clear();
+  if (f32info == nullptr || i32info == nullptr) return set_error(TOMO_ERR_ARG, "info arrays are null");
+  const Params P = read_params(f32info, i32info);
+  if (P.n_tri < 0 || P.n_vtx < 0 || P.n_ypr < 0) return set_error(TOMO_ERR_ARG, "negative size in Int32Info");
+  if (P.n_ypr > 0 && (YPR == nullptr || Mo == nullptr || Mss == nullptr || Vtc == nullptr))
+    return set_error(TOMO_ERR_ARG, "YPR or an output array is null");
+  if (P.n_tri > 0 && (tri == nullptr || vtx == nullptr || vtx_nrm == nullptr))
+    return set_error(TOMO_ERR_ARG, "mesh array is null");
+  if (P.n_tri > kStaticMaxTri)
+    return set_error(TOMO_ERR_CAPACITY, "tomoSweepStatic: " + std::to_string(P.n_tri) +
+                                            " triangles exceed the static limit of " + std::to_string(kStaticMaxTri));
+  if (P.n_vtx > kStaticMaxVtx)
+    return set_error(TOMO_ERR_CAPACITY, "tomoSweepStatic: " + std::to_string(P.n_vtx) +
+                                            " vertices exceed the static limit of " + std::to_string(kStaticMaxVtx));
+  for (int t = 0; t < P.n_tri * 3; t++)
+    if (tri[t] < 0 || tri[t] >= P.n_vtx) return set_error(TOMO_ERR_ARG, "triangle index out of range");
+  for (int k = 0; k < P.n_vtx * 3; k++)
+    if (!std::isfinite(vtx[k]) || !std::isfinite(vtx_nrm[k])) return set_error(TOMO_ERR_ARG, "non-finite vertex or normal");
+  for (int k = 0; k < P.n_ypr * 3; k++)
+    if (!std::isfinite(YPR[k])) return set_error(TOMO_ERR_ARG, "non-finite orientation");
+  if (!std::isfinite(P.dVoxel) || !std::isfinite(P.bed_outer) || !std::isfinite(P.theta_c) || P.bed_outer < 0.f ||
+      P.bed_outer > 1000.f)
+    return set_error(TOMO_ERR_ARG, "bad printer parameters");
+
+  Engine X;   // strip planning and kernel parameters only; reserves nothing
+  X.P = P;
+  X.nYPR = P.n_ypr;
+  float mn[3] = {1e5f, 1e5f, 1e5f}, mx[3] = {-1e5f, -1e5f, -1e5f};
+  for (int v = 0; v < P.n_vtx; v++)
+    for (int k = 0; k < 3; k++) {
+      const float d = vtx[v * 3 + k];
+      mn[k] = (mn[k] <= d) ? mn[k] : d;
+      mx[k] = (mx[k] >= d) ? mx[k] : d;
+    }
+  X.cx = (float)((double)(mn[0] + mx[0]) * 0.5);
+  X.cy = (float)((double)(mn[1] + mx[1]) * 0.5);
+  X.cz = (float)((double)(mn[2] + mx[2]) * 0.5);
+  X.G = X.choose_grid(vtx, P.n_vtx);
+  if (X.G > kStaticGrid)
+    return set_error(TOMO_ERR_CAPACITY, "tomoSweepStatic: the mesh footprint needs a slot grid of " +
+                                            std::to_string(X.G) + " columns, above the static limit of 256");
+
+  // what Calculate adds per bed pixel, folded (Engine::finalize_host)
+  int bedfold_n = 0;
+  g_static_bedfold[0] = 0.f;
+  auto finish = [&](int id, float vof, float vssf, float vtcf, int nbed) {
+    while (bedfold_n < nbed) { g_static_bedfold[bedfold_n + 1] = g_static_bedfold[bedfold_n] + (float)1 * P.bed_thickness; bedfold_n++; }
+    float vm[22] = {0};
+    vm[8] = vof; vm[4] = vssf; vm[2] = vtcf; vm[11] = g_static_bedfold[nbed];
+    vol_to_mass(P, vm);
+    Mo[id] = vm[16]; Mss[id] = vm[13]; Vtc[id] = vm[2];
+  };
+  if (P.n_ypr == 0) return 0;
+  if (P.n_tri == 0) {
+    for (int i = 0; i < P.n_ypr; i++) finish(i, 0.f, 0.f, 0.f, 0);
+    return first_optimal(P.n_ypr, Mss);
+  }
+
+  cudaStream_t st = (cudaStream_t)stream;
+  void* base = nullptr;
+  TOMO_TRY(static_arena(&base));
+  const StaticLayout L = static_layout((unsigned char*)base, P.n_vtx, P.n_tri);
+  int dev = 0, optin = 0;
+  TOMO_CUDA(cudaGetDevice(&dev));
+  TOMO_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  X.smem_optin = (size_t)optin;
+  X.plan_strips();
+  TOMO_TRY(X.configure());
+
+  for (int v = 0; v < P.n_vtx; v++) {
+    g_static_hpos[v] = make_float4(vtx[v * 3 + 0], vtx[v * 3 + 1], vtx[v * 3 + 2], 0.f);
+    g_static_hnrm[v] = make_float4(vtx_nrm[v * 3 + 0], vtx_nrm[v * 3 + 1], vtx_nrm[v * 3 + 2], 0.f);
+  }
+  for (int t = 0; t < P.n_tri; t++) g_static_htri[t] = make_int4(tri[t * 3 + 0], tri[t * 3 + 1], tri[t * 3 + 2], 0);
+  TOMO_CUDA(cudaMemcpyAsync(L.vpos, g_static_hpos, sizeof(float4) * P.n_vtx, cudaMemcpyHostToDevice, st));
+  TOMO_CUDA(cudaMemcpyAsync(L.vnrm, g_static_hnrm, sizeof(float4) * P.n_vtx, cudaMemcpyHostToDevice, st));
+  TOMO_CUDA(cudaMemcpyAsync(L.tri, g_static_htri, sizeof(int4) * P.n_tri, cudaMemcpyHostToDevice, st));
+  TOMO_CUDA(cudaMemcpyAsync(L.ori, g_static_hori, sizeof(g_static_hori), cudaMemcpyHostToDevice, st));
+
+  const int normal_cap = 4 * P.n_tri + 4096;
+  for (int first = 0; first < P.n_ypr; first += kStaticBatch) {
+    const int nb = std::min(kStaticBatch, P.n_ypr - first);
+    for (int o = 0; o < nb; o++)
+      rotation(YPR[(first + o) * 3 + 0], YPR[(first + o) * 3 + 1], YPR[(first + o) * 3 + 2], &g_static_hrot[o * 9]);
+    TOMO_CUDA(cudaMemcpyAsync(L.rot, g_static_hrot, sizeof(float) * 9 * nb, cudaMemcpyHostToDevice, st));
+    // out_nbed is accumulated with atomics; every other buffer the kernels
+    // read is written first by the batch itself (k_reset clears the rest)
+    TOMO_CUDA(cudaMemsetAsync(L.o_nbed, 0, sizeof(int) * nb, st));
+    X.choose_strips(0);
+    EngineParams p = X.base_params(0);
+    static_bind(p, L, nb, 0, normal_cap);
+    TOMO_CUDA(launch_batch(p, st, X.cfg[0].smem, nullptr));
+    TOMO_CUDA(launch_fold(p, st, nullptr));
+    TOMO_CUDA(cudaMemcpyAsync(g_static_hflags, L.o_flags, sizeof(int) * nb, cudaMemcpyDeviceToHost, st));
+    TOMO_CUDA(cudaStreamSynchronize(st));
+    // the re-run ladder of Engine::execute, per flagged slot
+    for (int o = 0; o < nb; o++) {
+      int fl = g_static_hflags[o];
+      if (fl & kFlagGrid) return set_error(TOMO_ERR_CAPACITY, "slot index outside the grid");
+      bool safe = (fl & (kFlagStray | kFlagBinCap)) != 0;
+      if (!safe && (fl & kFlagOverflow)) {
+        fl = static_rerun(X, L, o, 2, st);
+        if (fl < 0) return fl;
+        safe = (fl & (kFlagStray | kFlagBinCap | kFlagOverflow)) != 0;
+      }
+      if (safe) {
+        fl = static_rerun(X, L, o, 1, st);
+        if (fl < 0) return fl;
+        if (fl & kFlagSafeOverflow) {
+          fl = static_rerun(X, L, o, 3, st);
+          if (fl < 0) return fl;
+        }
+      }
+      if (fl & kFlagSafeOverflow) return set_error(TOMO_ERR_CAPACITY, "column strip exceeds shared memory");
+      if (fl & kFlagGrid) return set_error(TOMO_ERR_CAPACITY, "slot index outside the grid");
+      if (fl & (kFlagStray | kFlagOverflow | kFlagBinCap))
+        return set_error(TOMO_ERR_CAPACITY, "orientation unresolved after the re-runs");
+    }
+    TOMO_CUDA(cudaMemcpyAsync(g_static_hvof, L.o_vof, sizeof(float) * nb, cudaMemcpyDeviceToHost, st));
+    TOMO_CUDA(cudaMemcpyAsync(g_static_hvssf, L.o_vssf, sizeof(float) * nb, cudaMemcpyDeviceToHost, st));
+    TOMO_CUDA(cudaMemcpyAsync(g_static_hvtcf, L.o_vtcf, sizeof(float) * nb, cudaMemcpyDeviceToHost, st));
+    TOMO_CUDA(cudaMemcpyAsync(g_static_hnbed, L.o_nbed, sizeof(int) * nb, cudaMemcpyDeviceToHost, st));
+    TOMO_CUDA(cudaStreamSynchronize(st));
+    for (int o = 0; o < nb; o++) {
+      if (g_static_hnbed[o] < 0 || g_static_hnbed[o] > kStaticGrid * kStaticGrid)
+        return set_error(TOMO_ERR_CAPACITY, "bed pixel count outside the slot grid");
+      finish(first + o, g_static_hvof[o], g_static_hvssf[o], g_static_hvtcf[o], g_static_hnbed[o]);
+    }
+  }
+  return first_optimal(P.n_ypr, Mss);
+}

@@ -54,6 +54,7 @@ EXPORTS = [
     ("tomoProfile", ct.c_int, [ct.c_int, ct.c_int]),
     ("tomoGetKernelLog", ct.c_int, [_i64p, ct.POINTER(ct.c_double), _i64p, ct.c_int]),
     ("tomoColumnDump", ct.c_int, [ct.c_int, ct.c_int, _i32p, _u32p, _i16p]),
+    ("tomoSweepStatic", ct.c_int, [_f32p, _i32p, _f32p, _i32p, _f32p, _f32p, _f32p, _f32p, _f32p, ct.c_void_p]),
 ]
 
 _LIB: ct.CDLL | None = None
@@ -208,6 +209,19 @@ def sweep(mesh, ypr, opts) -> SweepResult:
                        r["VoF"], r["VssF"], r["VtcF"], r["n_bed"], r["flags"], r["entries"], r["columns"],
                        np.ctypeslib.as_array(L.getVolMassInfo(), shape=(22,)).copy(),
                        np.ctypeslib.as_array(L.getMat4x4(), shape=(16,)).copy().reshape(4, 4), pixels())
+
+
+def sweep_static(mesh, ypr, opts, stream: int | None = None) -> tuple[int, np.ndarray, np.ndarray, np.ndarray]:
+    """tomoSweepStatic: (optID, Mo, Mss, Vtc) without any allocation by the library."""
+    from .options import pack_info
+    f32, i32 = pack_info(opts, mesh, ypr.shape[0])
+    ypr, tri, vtx, vn, *_ = _arrays(mesh, ypr)
+    n = ypr.shape[0]
+    Mo, Mss, Vtc = (np.zeros(n, np.float32) for _ in range(3))
+    opt = _check(lib().tomoSweepStatic(_p(f32, _f32p), _p(i32, _i32p), _p(ypr, _f32p), _p(tri, _i32p),
+                                       _p(vtx, _f32p), _p(vn, _f32p), _p(Mo, _f32p), _p(Mss, _f32p),
+                                       _p(Vtc, _f32p), stream))
+    return opt, Mo, Mss, Vtc
 
 
 class Session:
