@@ -130,7 +130,8 @@ class ClockSampler:
 
 # ------------------------------------------------------------------ CPU baseline
 
-def cpu_baseline(mesh, ypr, opts, grid, budget_s: float, gpu_vss=None, threads: int | None = None):
+def cpu_baseline(mesh, ypr, opts, grid, budget_s: float, gpu_vss=None, threads: int | None = None,
+                 n: int | None = None):
     """The reference INT3 engine (oracle/_ref, built from the reference sources)
     -- or, if that library is absent, the oracle's C restatement -- on an
     evenly strided sample of the workload's orientations, all host threads."""
@@ -153,19 +154,21 @@ def cpu_baseline(mesh, ypr, opts, grid, budget_s: float, gpu_vss=None, threads: 
     if eng is None:
         eng, kind = Oracle(), "port"
     n_all = ypr.shape[0]
-    # calibrate on a small strided sample, then size the real one for ~budget_s
-    cal = max(threads, 8)
-    idx = np.linspace(0, n_all - 1, cal).astype(np.int64)
-    t0 = time.perf_counter()
-    eng.sweep(mesh, ypr[idx], opts, grid=grid, threads=threads)
-    per = (time.perf_counter() - t0) / cal
-    n = int(min(n_all, max(cal, budget_s / max(per, 1e-6))))
-    n = max(threads, (n // threads) * threads)
-    idx = np.linspace(0, n_all - 1, n).astype(np.int64)
-    t0 = time.perf_counter()
-    out = eng.sweep(mesh, ypr[idx], opts, grid=grid, threads=threads)
-    dt = time.perf_counter() - t0
-    res = {"value": n / dt, "unit": UNIT, "cores": int(threads), "kind": kind,
+    # grow a strided sample until one call takes at least half the budget
+    # (a call's fixed cost -- threads and their slot buffers -- makes small
+    # samples look slow, so the size is re-estimated from each larger call)
+    fixed = n is not None
+    n = min(n_all, n if fixed else max(threads, 8))
+    while True:
+        idx = np.linspace(0, n_all - 1, n).astype(np.int64)
+        t0 = time.perf_counter()
+        out = eng.sweep(mesh, ypr[idx], opts, grid=grid, threads=threads)
+        dt = time.perf_counter() - t0
+        if fixed or dt >= 0.5 * budget_s or n >= n_all:
+            break
+        n = int(min(n_all, max(2 * n, n * budget_s / max(dt, 1e-6))))
+        n = min(n_all, max(threads, (n // threads) * threads))
+    res = {"value": n / dt, "unit": UNIT, "cores": int(threads), "kind": kind, "n": n,
            "sample": f"{n} of the {n_all} orientations, evenly strided, one call, {dt:.1f} s"}
     if gpu_vss is not None and "Vss64" in out:
         res["sample_vss_bit_identical"] = bool(np.array_equal(out["Vss64"], gpu_vss[idx]))
@@ -180,13 +183,16 @@ def run_reference(args, rank):
     mesh, ypr, opts = workload(0)
     from tomo_shell2026_b200.meshgen import MeshArrays  # noqa: F401
     grid = _grid_for(mesh)
-    for _ in range(args.warmup):
-        cpu_baseline(mesh, ypr, opts, grid, budget_s=args.ref_step_s / 4)
+    # the first warm-up step sizes the sample (about ref_step_s of CPU work);
+    # every later step evaluates that same sample
+    n = None
+    for _ in range(max(1, args.warmup)):
+        n = cpu_baseline(mesh, ypr, opts, grid, budget_s=args.ref_step_s, n=n)["n"]
     vals = []
     last = None
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        last = cpu_baseline(mesh, ypr, opts, grid, budget_s=args.ref_step_s)
+        last = cpu_baseline(mesh, ypr, opts, grid, budget_s=args.ref_step_s, n=n)
         vals.append(last["value"])
     wall = time.perf_counter() - t0
     v = float(statistics.median(vals))
@@ -255,6 +261,8 @@ def run_ours(args, rank, world, local_rank):
     value = world * args.steps * n / (total_ms / 1000.0)
 
     # ---- e2e: reference C-ABI with host buffers (H2D + D2H inside)
+    for _ in range(args.warmup):
+        native.sweep(mesh, ypr, opts)
     e2e_s = []
     for _ in range(max(1, args.steps)):
         if dist:

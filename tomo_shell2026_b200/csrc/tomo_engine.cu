@@ -32,6 +32,9 @@ cudaError_t launch_batch(const EngineParams& p, cudaStream_t main, size_t strip_
 cudaError_t launch_fold(const EngineParams& p, cudaStream_t side, LaunchLog* L);
 cudaError_t launch_bin_count(const EngineParams& p, cudaStream_t main, LaunchLog* L);
 cudaError_t launch_after_count(const EngineParams& p, cudaStream_t main, size_t strip_smem, LaunchLog* L);
+cudaError_t launch_dump_scan(const int* cols8, int GG, int* off, int* totals, cudaStream_t s);
+cudaError_t launch_dump_gather(const int* cols8, const unsigned* keys64, const short* types64, int GG, const int* off,
+                               int* cols9, unsigned* keys, short* types, cudaStream_t s);
 
 namespace {
 
@@ -210,6 +213,9 @@ struct Engine {
   DevBuf<int> dump_cols;
   DevBuf<unsigned> dump_keys;
   DevBuf<short> dump_types;
+  DevBuf<int> dump_off, dump_tot, dump_ccols;
+  DevBuf<unsigned> dump_ckeys;
+  DevBuf<short> dump_ctypes;
 
   // host results of the last sweep
   Params P{};
@@ -257,6 +263,7 @@ struct Engine {
     o_vo.release(); o_vss.release(); o_vtc.release(); o_ent.release(); o_col.release();
     o_vof.release(); o_vssf.release(); o_vtcf.release(); o_nbed.release(); o_flags.release();
     dump_cols.release(); dump_keys.release(); dump_types.release();
+    dump_off.release(); dump_tot.release(); dump_ccols.release(); dump_ckeys.release(); dump_ctypes.release();
     log.destroy();
     if (main) { cudaStreamDestroy(main); main = nullptr; }
     if (side) { cudaStreamDestroy(side); side = nullptr; }
@@ -603,6 +610,51 @@ struct Engine {
   // One orientation with the dense per-column dump enabled (parity tests).
   int dump(int id, int c, int* cols8, unsigned* keys64, short* types64)
   {
+    const int fl = dump_device(id, c);
+    if (fl < 0) return fl;
+    const size_t GG = (size_t)G * G;
+    if (cols8) TOMO_CUDA(cudaMemcpyAsync(cols8, dump_cols.ptr, sizeof(int) * GG * 8, cudaMemcpyDeviceToHost, main));
+    if (keys64) TOMO_CUDA(cudaMemcpyAsync(keys64, dump_keys.ptr, sizeof(unsigned) * GG * 64, cudaMemcpyDeviceToHost, main));
+    if (types64) TOMO_CUDA(cudaMemcpyAsync(types64, dump_types.ptr, sizeof(short) * GG * 64, cudaMemcpyDeviceToHost, main));
+    TOMO_CUDA(cudaStreamSynchronize(main));
+    return fl;
+  }
+
+  // The same dump compacted on the device to the occupied columns:
+  // cols9[n_occ][9] = slot id + the 8 dump fields, keys/types = each occupied
+  // column's kept keys and types, concatenated in slot order.
+  int dump_compact(int id, int c, std::vector<int>& cols9, std::vector<unsigned>& keys, std::vector<short>& types)
+  {
+    const int fl = dump_device(id, c);
+    if (fl < 0) return fl;
+    const int GG = G * G;
+    TOMO_CUDA(dump_off.reserve((size_t)GG * 2));
+    TOMO_CUDA(dump_tot.reserve(2));
+    TOMO_CUDA(launch_dump_scan(dump_cols.ptr, GG, dump_off.ptr, dump_tot.ptr, main));
+    int tot[2] = {0, 0};
+    TOMO_CUDA(cudaMemcpyAsync(tot, dump_tot.ptr, sizeof(tot), cudaMemcpyDeviceToHost, main));
+    TOMO_CUDA(cudaStreamSynchronize(main));
+    TOMO_CUDA(dump_ccols.reserve((size_t)tot[0] * 9));
+    TOMO_CUDA(dump_ckeys.reserve((size_t)tot[1]));
+    TOMO_CUDA(dump_ctypes.reserve((size_t)tot[1]));
+    TOMO_CUDA(launch_dump_gather(dump_cols.ptr, dump_keys.ptr, dump_types.ptr, GG, dump_off.ptr, dump_ccols.ptr,
+                                 dump_ckeys.ptr, dump_ctypes.ptr, main));
+    cols9.resize((size_t)tot[0] * 9);
+    keys.resize((size_t)tot[1]);
+    types.resize((size_t)tot[1]);
+    if (tot[0]) TOMO_CUDA(cudaMemcpyAsync(cols9.data(), dump_ccols.ptr, sizeof(int) * cols9.size(), cudaMemcpyDeviceToHost, main));
+    if (tot[1]) {
+      TOMO_CUDA(cudaMemcpyAsync(keys.data(), dump_ckeys.ptr, sizeof(unsigned) * keys.size(), cudaMemcpyDeviceToHost, main));
+      TOMO_CUDA(cudaMemcpyAsync(types.data(), dump_ctypes.ptr, sizeof(short) * types.size(), cudaMemcpyDeviceToHost, main));
+    }
+    TOMO_CUDA(cudaStreamSynchronize(main));
+    return fl;
+  }
+
+  // Runs one orientation in strip configuration c with the dense dump on;
+  // returns its status flags.
+  int dump_device(int id, int c)
+  {
     if (id < 0 || id >= nYPR) return set_error(TOMO_ERR_ARG, "orientation index out of range");
     if (P.n_tri == 0) return set_error(TOMO_ERR_ARG, "empty mesh");
     if (c < 0 || c > 3) return set_error(TOMO_ERR_ARG, "bad strip configuration");
@@ -635,12 +687,9 @@ struct Engine {
       TOMO_CUDA(launch_after_count(p, main, smem, &log));
     }
     TOMO_CUDA(launch_fold(p, main, &log));
-    if (cols8) TOMO_CUDA(cudaMemcpyAsync(cols8, dump_cols.ptr, sizeof(int) * GG * 8, cudaMemcpyDeviceToHost, main));
-    if (keys64) TOMO_CUDA(cudaMemcpyAsync(keys64, dump_keys.ptr, sizeof(unsigned) * GG * 64, cudaMemcpyDeviceToHost, main));
-    if (types64) TOMO_CUDA(cudaMemcpyAsync(types64, dump_types.ptr, sizeof(short) * GG * 64, cudaMemcpyDeviceToHost, main));
-    TOMO_CUDA(cudaStreamSynchronize(main));
     int fl = 0;
-    TOMO_CUDA(cudaMemcpy(&fl, o_flags.ptr + id, sizeof(int), cudaMemcpyDeviceToHost));
+    TOMO_CUDA(cudaMemcpyAsync(&fl, o_flags.ptr + id, sizeof(int), cudaMemcpyDeviceToHost, main));
+    TOMO_CUDA(cudaStreamSynchronize(main));
     return fl;
   }
 
@@ -743,37 +792,49 @@ int export_best(Engine& E, int id, std::vector<short>* pix, int* npix, float* vm
 {
   const int G = E.G;
   const size_t GG = (size_t)G * G;
-  std::vector<int> cols(GG * 8);
-  std::vector<unsigned> keys(GG * 64);
-  std::vector<short> types(GG * 64);
+  std::vector<int> cols;
+  std::vector<unsigned> keys;
+  std::vector<short> types;
   int fl = -1;
   for (int c : {0, 1, 3}) {
-    fl = E.dump(id, c, cols.data(), keys.data(), types.data());
+    fl = E.dump_compact(id, c, cols, keys, types);
     if (fl < 0) return fl;
     if (!(fl & (kFlagStray | kFlagOverflow | kFlagBinCap | kFlagSafeOverflow))) break;
   }
   if (fl & (kFlagStray | kFlagOverflow | kFlagBinCap | kFlagSafeOverflow | kFlagGrid))
     return set_error(TOMO_ERR_CAPACITY, "best orientation could not be exported");
-  std::vector<std::vector<SlotRow>> rows(GG);
+  // occupied columns in slot order: rows[rbeg[j] .. rbeg[j+1]) plus an
+  // optional bed row (bed_row[j]); bed-only columns listed separately
+  const int nocc = (int)(cols.size() / 9);
+  std::vector<SlotRow> rows;
+  rows.reserve(keys.size() + 2 * (size_t)nocc);
+  std::vector<int> rbeg((size_t)nocc + 1, 0);
+  std::vector<int> colidx(GG, -1);
+  std::vector<uint8_t> bed_row((size_t)nocc, 0);
   std::vector<uint8_t> bf(GG, (uint8_t)(kBfPoss | kBfLand));
   int minX = G, minY = G, maxX = -1, maxY = -1;
-  for (size_t sl = 0; sl < GG; sl++) {
-    const int* c = &cols[sl * 8];
-    const int nd = c[0], nfin = c[1];
-    if (nd == 0) continue;
-    const int x = (int)(sl / G), y = (int)(sl % G);
+  size_t k0 = 0;
+  for (int j = 0; j < nocc; j++) {
+    const int* c = &cols[(size_t)j * 9];
+    const int sl = c[0], nd = c[1], nfin = c[2];
+    const int x = sl / G, y = sl % G;
     minX = std::min(minX, x); maxX = std::max(maxX, x); minY = std::min(minY, y); maxY = std::max(maxY, y);
-    auto& r = rows[sl];
-    for (int i = 0; i < nd && i < 64; i++) {
-      const unsigned k = keys[sl * 64 + i];
-      r.push_back({nd > 1 ? types[sl * 64 + i] : (short)0, (short)((int)(k >> 16) - 32768), (short)((int)(k & 0xFFFFu) - 32768)});
+    rbeg[j] = (int)rows.size();
+    const int n = std::min(nd, 64);
+    for (int i = 0; i < n; i++) {
+      const unsigned k = keys[k0 + i];
+      rows.push_back({nd > 1 ? types[k0 + i] : (short)0, (short)((int)(k >> 16) - 32768), (short)((int)(k & 0xFFFFu) - 32768)});
     }
+    k0 += (size_t)n;
     const int extra = nfin - nd;
-    if (extra == 2) { r.push_back({(short)kSSA, 0, 0}); r.push_back({(short)kNVA, 0, 0}); }
-    else if (extra == 1) r.push_back({(short)c[6], 0, 0});
-    bf[sl] = (uint8_t)c[7];
+    if (extra == 2) { rows.push_back({(short)kSSA, 0, 0}); rows.push_back({(short)kNVA, 0, 0}); }
+    else if (extra == 1) rows.push_back({(short)c[7], 0, 0});
+    bf[sl] = (uint8_t)c[8];
+    colidx[sl] = j;
   }
+  rbeg[nocc] = (int)rows.size();
   // bed pixels, in the reference's scan order
+  std::vector<int> bed_only;
   if (E.P.bed_type != kBedNone && maxX >= 0 && (int)E.P.bed_outer > 0) {
     const int m = (int)E.P.bed_outer + 1;
     const int bx0 = std::max(minX - m, 0), bx1 = std::min(maxX + m + 1, G);
@@ -783,26 +844,30 @@ int export_best(Engine& E, int id, std::vector<short>* pix, int* npix, float* vm
         const size_t sl = (size_t)X * G + Y;
         const uint8_t f = bf[sl];
         if (!((f & kBfPoss) && (f & kBfLand)) || !host_bed_candidate(E, bf, X, Y)) continue;
-        auto& r = rows[sl];
+        const int j = colidx[sl];
+        if (j < 0) { bed_only.push_back((int)sl); continue; }
         bool merged = false;
-        for (auto& q : r)
-          if (q.z == 1 && q.nz == 0) { q.type |= (short)kBed; merged = true; break; }
-        if (!merged) r.push_back({(short)kBed, 1, 0});
+        for (int r = rbeg[j]; r < rbeg[j + 1]; r++)
+          if (rows[r].z == 1 && rows[r].nz == 0) { rows[r].type |= (short)kBed; merged = true; break; }
+        if (!merged) bed_row[j] = 1;
       }
   }
-  // render pixels per type (slotsToPxls) and the support pixels (GetSSPixels)
+  // render pixels per type (slotsToPxls), the support pixels (GetSSPixels)
+  // and the float folds of Calculate, over the final slots in ascending order
   for (int k = 0; k < 11; k++) pix[k].clear();
-  for (size_t sl = 0; sl < GG; sl++) {
-    if (rows[sl].empty()) continue;
+  float va = 0.f, vb = 0.f, vnv = 0.f, vtc = 0.f, vbed = 0.f;
+  const SlotRow bed_px = {(short)kBed, 1, 0};
+  auto column = [&](int sl, const SlotRow* r, int n, bool extra_bed) {
     const short x = (short)(sl / G), y = (short)(sl % G);
-    for (const auto& q : rows[sl])
+    int sa = 0, sb = 0, snvb = 0, snva = 0, stc = 0, sbed = 0;
+    int ss0 = -1, ss1 = -1;
+    for (int i = 0; i < n + (extra_bed ? 1 : 0); i++) {
+      const SlotRow& q = i < n ? r[i] : bed_px;
       for (int k = 0; k < 11; k++)
         if (k != 4 && (q.type & (1 << k))) {
           const short px[6] = {x, y, q.z, 0, 0, q.nz};
           pix[k].insert(pix[k].end(), px, px + 6);
         }
-    int ss0 = -1, ss1 = -1;
-    for (const auto& q : rows[sl]) {
       if (q.type & kSSB) ss0 = q.z;
       if (q.type & kSSA) ss1 = q.z;
       if (ss0 > -1 && ss1 > -1) {
@@ -812,15 +877,6 @@ int export_best(Engine& E, int id, std::vector<short>* pix, int* npix, float* vm
         }
         ss0 = ss1 = -1;
       }
-    }
-  }
-  for (int k = 0; k < 11; k++) npix[k] = (int)(pix[k].size() / 6);
-  // Calculate: float folds over the occupied slots in ascending order
-  float va = 0.f, vb = 0.f, vnv = 0.f, vtc = 0.f, vbed = 0.f;
-  for (size_t sl = 0; sl < GG; sl++) {
-    if (rows[sl].empty()) continue;
-    int sa = 0, sb = 0, snvb = 0, snva = 0, stc = 0, sbed = 0;
-    for (const auto& q : rows[sl]) {
       if (q.type & kAl) sa += q.z;
       if (q.type & kBe) sb += q.z;
       if (q.type & kNVB) snvb += q.z;
@@ -830,7 +886,14 @@ int export_best(Engine& E, int id, std::vector<short>* pix, int* npix, float* vm
     }
     va += (float)sa; vb += (float)sb; vnv += (float)(snvb - snva); vtc += (float)stc;
     vbed += (float)sbed * E.P.bed_thickness;
+  };
+  size_t b = 0;
+  for (int j = 0; j <= nocc; j++) {
+    const int sl = j < nocc ? cols[(size_t)j * 9] : INT_MAX;
+    while (b < bed_only.size() && bed_only[b] < sl) { column(bed_only[b], nullptr, 0, true); b++; }
+    if (j < nocc) column(sl, rows.data() + rbeg[j], rbeg[j + 1] - rbeg[j], bed_row[j] != 0);
   }
+  for (int k = 0; k < 11; k++) npix[k] = (int)(pix[k].size() / 6);
   vm[0] = va; vm[1] = vb; vm[2] = vtc; vm[3] = vnv; vm[11] = vbed;
   return 0;
 }

@@ -1172,6 +1172,65 @@ __global__ void __launch_bounds__(128) k_fold(EngineParams p)
   }
 }
 
+// ---------------------------------------------------------------- dump compaction
+// The dense per-column dump ([G*G][8] fields, [G*G][64] keys and types) is
+// mostly empty; these two kernels compact it to the occupied columns before
+// it crosses PCIe.  off[2*sl] / off[2*sl+1] = exclusive offsets of column
+// sl among the occupied columns / the kept keys; totals = both counts.
+
+__global__ void __launch_bounds__(1024) k_dump_scan(const int* cols8, int GG, int* off, int* totals)
+{
+  __shared__ long long wt[32];
+  const int per = (GG + blockDim.x - 1) / blockDim.x;
+  const int b = threadIdx.x * per;
+  auto item = [&](int sl) -> long long {
+    const int nd = cols8[(size_t)sl * 8];
+    return nd > 0 ? (1ll << 32) + (nd < 64 ? nd : 64) : 0ll;
+  };
+  long long local = 0;
+  for (int i = 0; i < per; i++) if (b + i < GG) local += item(b + i);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  long long x = local;
+  for (int d = 1; d < 32; d <<= 1) { const long long y = __shfl_up_sync(0xFFFFFFFFu, x, d); if (lane >= d) x += y; }
+  if (lane == 31) wt[wid] = x;
+  __syncthreads();
+  if (wid == 0) {
+    long long t = wt[lane];
+    for (int d = 1; d < 32; d <<= 1) { const long long y = __shfl_up_sync(0xFFFFFFFFu, t, d); if (lane >= d) t += y; }
+    wt[lane] = t;
+  }
+  __syncthreads();
+  long long run = ((wid > 0) ? wt[wid - 1] : 0ll) + x - local;
+  for (int i = 0; i < per; i++) {
+    const int sl = b + i;
+    if (sl >= GG) break;
+    off[2 * sl] = (int)(run >> 32);
+    off[2 * sl + 1] = (int)(run & 0xFFFFFFFFll);
+    run += item(sl);
+  }
+  if (threadIdx.x == 0) {
+    totals[0] = (int)(wt[31] >> 32);
+    totals[1] = (int)(wt[31] & 0xFFFFFFFFll);
+  }
+}
+
+__global__ void __launch_bounds__(256) k_dump_gather(const int* cols8, const unsigned* keys64, const short* types64,
+                                                     int GG, const int* off, int* cols9, unsigned* keys, short* types)
+{
+  for (int sl = blockIdx.x * blockDim.x + threadIdx.x; sl < GG; sl += gridDim.x * blockDim.x) {
+    const int nd = cols8[(size_t)sl * 8];
+    if (nd <= 0) continue;
+    const int c = off[2 * sl], k = off[2 * sl + 1];
+    cols9[(size_t)c * 9] = sl;
+    for (int f = 0; f < 8; f++) cols9[(size_t)c * 9 + 1 + f] = cols8[(size_t)sl * 8 + f];
+    const int n = nd < 64 ? nd : 64;
+    for (int i = 0; i < n; i++) {
+      keys[(size_t)k + i] = keys64[(size_t)sl * 64 + i];
+      types[(size_t)k + i] = types64[(size_t)sl * 64 + i];
+    }
+  }
+}
+
 }  // namespace tomo
 
 // ---------------------------------------------------------------- launchers
@@ -1253,6 +1312,20 @@ cudaError_t launch_batch(const EngineParams& p, cudaStream_t main, size_t strip_
   cudaError_t e = launch_bin_count(p, main, L);
   if (e != cudaSuccess) return e;
   return launch_after_count(p, main, strip_smem, L);
+}
+
+cudaError_t launch_dump_scan(const int* cols8, int GG, int* off, int* totals, cudaStream_t s)
+{
+  k_dump_scan<<<1, 1024, 0, s>>>(cols8, GG, off, totals);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_dump_gather(const int* cols8, const unsigned* keys64, const short* types64, int GG, const int* off,
+                               int* cols9, unsigned* keys, short* types, cudaStream_t s)
+{
+  const int blocks = (GG + 255) / 256 < 148 * 8 ? (GG + 255) / 256 : 148 * 8;
+  k_dump_gather<<<blocks > 0 ? blocks : 1, 256, 0, s>>>(cols8, keys64, types64, GG, off, cols9, keys, types);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_fold(const EngineParams& p, cudaStream_t side, LaunchLog* L)
