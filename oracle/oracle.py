@@ -34,8 +34,12 @@ def _p(a, t):
 
 
 def _inputs(mesh, ypr, opts):
+    """C-ABI argument arrays; ``opts`` is PrintOptions or a ready (Float32Info, Int32Info) pair."""
     from tomo_shell2026_b200.options import pack_info
-    f32, i32 = pack_info(opts, mesh, ypr.shape[0])
+    if isinstance(opts, tuple):
+        f32, i32 = (np.ascontiguousarray(opts[0], np.float32), np.ascontiguousarray(opts[1], np.int32))
+    else:
+        f32, i32 = pack_info(opts, mesh, ypr.shape[0])
     return (f32, i32, np.ascontiguousarray(ypr, np.float32), np.ascontiguousarray(mesh.faces, np.int32),
             np.ascontiguousarray(mesh.vertices, np.float32), np.ascontiguousarray(mesh.vertex_normals, np.float32),
             np.ascontiguousarray(mesh.face_normals, np.float32),

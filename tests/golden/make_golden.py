@@ -63,8 +63,51 @@ def cases():
                                                           bed_outer=2.0, bed_thickness=0.97)
 
 
+def manager_parts():
+    """Two parts for the reference-compatible front-end: a closed solid and
+    an open one (its top cap removed), which switches the shell mode on."""
+    from tomo_shell2026_b200.cfms_tomo import TriMesh
+    a = meshgen.small_solid(2, with_hull=False)
+    b = meshgen.small_solid(3, with_hull=False)
+    cz = b.vertices[b.faces].mean(1)[:, 2]
+    keep = cz < np.quantile(cz, 0.85)
+    parts = []
+    for name, v, f in (("closed", a.vertices, a.faces), ("open", b.vertices, b.faces[keep])):
+        m = meshgen.mesh_from_arrays(v, f, name, with_hull=False)
+        parts.append(TriMesh(m.vertices.astype(np.float64), m.faces, vertex_normals=m.vertex_normals,
+                             process=False, name=name))
+    return parts
+
+
+def make_manager(ref):
+    """TomoManager over the two parts, evaluated by the reference engine with
+    exactly the arrays TomoDLLInterface packs (theta_YP = 30: 13 x 13 YPR)."""
+    from tomo_shell2026_b200.cfms_tomo import SlicingOptions, TomoDLLInterface
+    s_o = SlicingOptions()
+    s_o.theta_YP = 30
+    s_o.bVerbose = False
+    itf = TomoDLLInterface("Tomo_Shell2026.dll", s_o, True, True)
+    out = {"YPR": itf.YPR}
+    for k, tm in enumerate(manager_parts()):
+        itf.bShellMesh = s_o.bShellMesh and not tm.is_watertight
+        itf.pack(tm, itf.YPR.shape[0], False)
+        info = (itf.Float32Info.copy(), itf.Int32Info.copy())
+        arrays = tm.to_arrays(with_hull=True)
+        sw = ref.sweep(arrays, itf.YPR, info, grid=256, threads=8)
+        ex = ref.pixels(arrays, itf.YPR, info, int(sw["optID"]), grid=256)
+        out.update({f"p{k}_vertices": arrays.vertices, f"p{k}_faces": arrays.faces,
+                    f"p{k}_vertex_normals": arrays.vertex_normals, f"p{k}_f32info": info[0], f"p{k}_i32info": info[1],
+                    f"p{k}_Mss": sw["Mss"], f"p{k}_Mo": sw["Mo"], f"p{k}_optID": np.int32(sw["optID"]),
+                    f"p{k}_SS": ex["pixels"][4], f"p{k}_Bed": ex["pixels"][5], f"p{k}_mat16": ex["mat16"]})
+    itf.free()
+    np.savez_compressed(OUT / "manager_two_parts.npz", **out)
+    print(f"manager_two_parts: {itf.YPR.shape[0]} orientations per part, "
+          f"{(OUT / 'manager_two_parts.npz').stat().st_size / 1024:.0f} KB")
+
+
 def main():
     ref = RefEngine()
+    make_manager(ref)
     for name, mesh, ypr, opts in cases():
         f32, i32 = pack_info(opts, mesh, ypr.shape[0])
         out = ref.sweep(mesh, ypr, opts, grid=256, threads=8)

@@ -10,7 +10,8 @@ import pytest
 from tomo_shell2026_b200.meshgen import MeshArrays
 from tomo_shell2026_b200.options import PrintOptions
 
-GOLDEN = sorted((Path(__file__).parent / "golden").glob("*.npz"))
+# per-case sweep fixtures (manager_*.npz belong to the front-end tests)
+GOLDEN = sorted(p for p in (Path(__file__).parent / "golden").glob("*.npz") if not p.name.startswith("manager_"))
 
 
 def load_case(path):
