@@ -45,11 +45,13 @@ PITCH = np.arange(0, 61, 1)
 L2_BYTES = 126 * 1024 * 1024
 
 
-def workload(seed: int):
+def workload(seed: int, max_orientations: int = 0):
     from tomo_shell2026_b200 import meshgen
     from tomo_shell2026_b200.options import PrintOptions
     mesh = meshgen.solid_82k(seed)
     ypr = meshgen.ypr_grid(YAW, PITCH)
+    if max_orientations > 0:
+        ypr = np.ascontiguousarray(ypr[:max_orientations])
     opts = PrintOptions(explicit_ss=True)
     return mesh, ypr, opts
 
@@ -180,7 +182,7 @@ def cpu_baseline(mesh, ypr, opts, grid, budget_s: float, gpu_vss=None, threads: 
 def run_reference(args, rank):
     if rank != 0:
         return 0
-    mesh, ypr, opts = workload(0)
+    mesh, ypr, opts = workload(0, args.max_orientations)
     from tomo_shell2026_b200.meshgen import MeshArrays  # noqa: F401
     grid = _grid_for(mesh)
     # the first warm-up step sizes the sample (about ref_step_s of CPU work);
@@ -224,7 +226,7 @@ def run_ours(args, rank, world, local_rank):
     dist = None
     if world > 1:
         import torch.distributed as dist
-    mesh, ypr, opts = workload(rank)
+    mesh, ypr, opts = workload(rank, args.max_orientations)
     n = ypr.shape[0]
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
@@ -362,6 +364,8 @@ def main():
     ap.add_argument("--cpu-budget-s", type=float, default=15.0)
     ap.add_argument("--ref-step-s", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--max-orientations", type=int, default=0,
+                    help="keep only the first N orientations (small profiling cases; 0 = the whole grid)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
