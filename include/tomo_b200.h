@@ -131,6 +131,36 @@ int tomoGridSize(void);
  * Returns the orientation's status flags (>= 0) or a negative error. */
 int tomoColumnDump(int ypr_index, int safe_mode, int* cols8, unsigned* keys64, short* types64);
 
+/* ---- multi-mesh batch (the additive TomoSh_CUDA_Batch export; no reference
+ * counterpart, the reference front-end loops over parts calling TomoSh_CUDA,
+ * cfms_tomo/__init__.py:26-30).  Each argument is an array of n_mesh pointers
+ * to that mesh's TomoSh_CUDA argument; meshes may differ in triangle count,
+ * printer options and orientation list.  tomoBatchPrepare uploads every mesh
+ * and picks each size class's strip configuration by timing candidates
+ * (autotuner); tomoBatchRun sweeps all meshes -- with use_graph, as one CUDA
+ * graph captured on the first run and replayed after -- re-runs flagged
+ * orientations per mesh and leaves per-mesh results equal to TomoSh_CUDA on
+ * that mesh alone; device_ms receives the device time of the sweep.
+ * tomoBatchResults copies mesh `mesh`'s per-orientation results (any pointer
+ * may be null) and returns its optID.  TomoSh_CUDA_Batch = prepare + run with
+ * the graph + optIDs[n_mesh]. */
+int tomoBatchPrepare(int n_mesh, const float* const* f32info, const int* const* i32info, const float* const* YPR,
+                     const int* const* tri, const float* const* vtx, const float* const* vtx_nrm);
+int tomoBatchRun(int use_graph, float* device_ms);
+int tomoBatchResults(int mesh, float* Mo, float* Mss, float* Vtc, long long* vo64, long long* vss64, long long* vtc64);
+int TomoSh_CUDA_Batch(int n_mesh, const float* const* f32info, const int* const* i32info, const float* const* YPR,
+                      const int* const* tri, const float* const* vtx, const float* const* vtx_nrm, int* optIDs);
+/* out[0..7] = meshes, orientations, graph nodes, kernels per graph launch,
+ * size classes tuned by the last prepare, size classes tuned so far,
+ * orientations re-run, device time of the last run in microseconds */
+int tomoBatchStats(long long* out, int n);
+/* out4 = orientations per batch, normal-CTA shared-memory budget (0 = 72 KB),
+ * strip height, slot-grid edge chosen for mesh `mesh` */
+int tomoBatchConfig(int mesh, int* out4);
+/* key 1: autotune on/off (default 1); key 2: autotune sample orientations (default 512) */
+int tomoBatchSetOption(int key, int value);
+void tomoBatchRelease(void);
+
 /* Allocation-free form of TomoSh_CUDA for small meshes.  No counterpart in the
  * reference.  Same inputs as TomoSh_CUDA; Mo, Mss and Vtc are caller-owned
  * host arrays of nYPR floats that receive what getMo/getMss/getVtc return

@@ -20,6 +20,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -187,55 +188,25 @@ struct BatchSet {   // per-batch buffers read by the fold, double-buffered
 
 // ------------------------------------------------ engine
 
-struct Engine {
+// Streams and batch work buffers, shared by every mesh of a multi-mesh sweep
+// (one Workspace per Engine for the single-mesh C-ABI).  Buffers only grow.
+struct Workspace {
   int device = -1;
   cudaStream_t main = nullptr, side = nullptr;
   cudaEvent_t ev_ready = nullptr;
   size_t smem_optin = 0;
-
-  // mesh and orientations
-  DevBuf<float4> vpos, vnrm;
-  DevBuf<int4> tri;
-  DevBuf<float> rot;
-  DevBuf<int> ori;
-  // batch work buffers
   DevBuf<float4> xf;
   DevBuf<unsigned> minkey;
   DevBuf<unsigned> trange;
   DevBuf<int> bin_off, bin_cur, bins, bbox;
   DevBuf<uint8_t> bedf;
   BatchSet set[2];
-  // outputs
-  DevBuf<long long> o_vo, o_vss, o_vtc, o_ent, o_col;
-  DevBuf<float> o_vof, o_vssf, o_vtcf;
-  DevBuf<int> o_nbed, o_flags;
-  // dump
   DevBuf<int> dump_cols;
   DevBuf<unsigned> dump_keys;
   DevBuf<short> dump_types;
   DevBuf<int> dump_off, dump_tot, dump_ccols;
   DevBuf<unsigned> dump_ckeys;
   DevBuf<short> dump_ctypes;
-
-  // host results of the last sweep
-  Params P{};
-  int nYPR = 0, G = 0, H = 0, S = 0, ent_cap = 0;
-  int batch = 128;
-  int force_h = 0;        // test hook: strip height override
-  int force_safe = 0;     // test hook: run every orientation in safe mode
-  int normal_smem = 0;    // shared-memory budget of a normal strip CTA (0 = 72 KB)
-  int export_pixels = 1;  // rebuild the best orientation's pixels and vm_info (TomoSh_CUDA tail)
-  float cx = 0, cy = 0, cz = 0;
-  std::vector<float> h_rot;
-  std::vector<long long> vo64, vss64, vtc64, entries, columns;
-  std::vector<float> vof, vssf, vtcf, Mo, Mss, Vtc;
-  std::vector<int> nbed, flags;
-  float volmass[22] = {0};
-  float mat4x4[16] = {0};
-  double last_kernel_ms = 0.0;
-  int n_safe = 0;
-  int n_redo[4] = {0, 0, 0, 0};
-  int H_sweep = 0;        // strip height of the last normal sweep
   LaunchLog log;
 
   int init()
@@ -256,12 +227,9 @@ struct Engine {
 
   void release()
   {
-    vpos.release(); vnrm.release(); tri.release(); rot.release(); ori.release();
     xf.release(); minkey.release(); trange.release(); bin_off.release(); bin_cur.release(); bins.release();
     bbox.release(); bedf.release();
     for (auto& s : set) { s.acc.release(); s.flags.release(); s.foldcnt.release(); s.foldv.release(); s.foldmeta.release(); }
-    o_vo.release(); o_vss.release(); o_vtc.release(); o_ent.release(); o_col.release();
-    o_vof.release(); o_vssf.release(); o_vtcf.release(); o_nbed.release(); o_flags.release();
     dump_cols.release(); dump_keys.release(); dump_types.release();
     dump_off.release(); dump_tot.release(); dump_ccols.release(); dump_ckeys.release(); dump_ctypes.release();
     log.destroy();
@@ -269,6 +237,88 @@ struct Engine {
     if (side) { cudaStreamDestroy(side); side = nullptr; }
     if (ev_ready) { cudaEventDestroy(ev_ready); ev_ready = nullptr; }
     for (auto& s : set) if (s.folded) { cudaEventDestroy(s.folded); s.folded = nullptr; }
+  }
+};
+
+// One mesh: its device arrays, orientations, outputs and host results; the
+// streams and work buffers are the Workspace's (bound by reference).
+struct Engine {
+  Workspace& W;
+  bool owns_ws;
+  int& device;
+  cudaStream_t& main;
+  cudaStream_t& side;
+  cudaEvent_t& ev_ready;
+  size_t& smem_optin;
+  DevBuf<float4>& xf;
+  DevBuf<unsigned>& minkey;
+  DevBuf<unsigned>& trange;
+  DevBuf<int>& bin_off;
+  DevBuf<int>& bin_cur;
+  DevBuf<int>& bins;
+  DevBuf<int>& bbox;
+  DevBuf<uint8_t>& bedf;
+  BatchSet (&set)[2];
+  DevBuf<int>& dump_cols;
+  DevBuf<unsigned>& dump_keys;
+  DevBuf<short>& dump_types;
+  DevBuf<int>& dump_off;
+  DevBuf<int>& dump_tot;
+  DevBuf<int>& dump_ccols;
+  DevBuf<unsigned>& dump_ckeys;
+  DevBuf<short>& dump_ctypes;
+  LaunchLog& log;
+
+  explicit Engine(Workspace& w, bool owns = false)
+      : W(w), owns_ws(owns), device(w.device), main(w.main), side(w.side), ev_ready(w.ev_ready),
+        smem_optin(w.smem_optin), xf(w.xf), minkey(w.minkey), trange(w.trange), bin_off(w.bin_off),
+        bin_cur(w.bin_cur), bins(w.bins), bbox(w.bbox), bedf(w.bedf), set(w.set), dump_cols(w.dump_cols),
+        dump_keys(w.dump_keys), dump_types(w.dump_types), dump_off(w.dump_off), dump_tot(w.dump_tot),
+        dump_ccols(w.dump_ccols), dump_ckeys(w.dump_ckeys), dump_ctypes(w.dump_ctypes), log(w.log)
+  {
+  }
+  Engine(const Engine&) = delete;
+  Engine& operator=(const Engine&) = delete;
+
+  // mesh and orientations
+  DevBuf<float4> vpos, vnrm;
+  DevBuf<int4> tri;
+  DevBuf<float> rot;
+  DevBuf<int> ori;
+  // outputs
+  DevBuf<long long> o_vo, o_vss, o_vtc, o_ent, o_col;
+  DevBuf<float> o_vof, o_vssf, o_vtcf;
+  DevBuf<int> o_nbed, o_flags;
+
+  // host results of the last sweep
+  Params P{};
+  int nYPR = 0, G = 0, H = 0, S = 0, ent_cap = 0;
+  int batch = 128;
+  int force_h = 0;        // test hook: strip height override
+  int force_safe = 0;     // test hook: run every orientation in safe mode
+  int normal_smem = 0;    // shared-memory budget of a normal strip CTA (0 = 72 KB)
+  int export_pixels = 1;  // rebuild the best orientation's pixels and vm_info (TomoSh_CUDA tail)
+  float cx = 0, cy = 0, cz = 0;
+  std::vector<float> h_rot;
+  std::vector<long long> vo64, vss64, vtc64, entries, columns;
+  std::vector<float> vof, vssf, vtcf, Mo, Mss, Vtc;
+  std::vector<int> nbed, flags;
+  float volmass[22] = {0};
+  float mat4x4[16] = {0};
+  double last_kernel_ms = 0.0;
+  int n_safe = 0;
+  int n_redo[4] = {0, 0, 0, 0};
+  int H_sweep = 0;        // strip height of the last normal sweep
+
+  int init() { return W.init(); }
+
+  // Frees this mesh's buffers, and the workspace when the engine owns it.
+  void release()
+  {
+    vpos.release(); vnrm.release(); tri.release(); rot.release(); ori.release();
+    o_vo.release(); o_vss.release(); o_vtc.release(); o_ent.release(); o_col.release();
+    o_vof.release(); o_vssf.release(); o_vtcf.release(); o_nbed.release(); o_flags.release();
+    if (owns_ws) W.release();
   }
 
   // Grid edge: the reference grid is 256 x 256 (STomoVoxelSpaceInfo.h:10).
@@ -461,25 +511,28 @@ struct Engine {
     p.foldcnt = set[which].foldcnt.ptr; p.foldv = set[which].foldv.ptr; p.foldmeta = set[which].foldmeta.ptr;
   }
 
-  // All orientations in configuration 0, asynchronously on `main`.
-  int sweep_device()
+  // All orientations in configuration 0, asynchronously on `main`.  With
+  // `ids`, only the n_ids orientations listed in that device array.
+  int sweep_device(const int* ids = nullptr, int n_ids = 0)
   {
-    if (nYPR == 0 || P.n_tri == 0) return 0;
+    const int n = ids ? n_ids : nYPR;
+    if (n == 0 || P.n_tri == 0) return 0;
     choose_strips(0);
     H_sweep = H;
     TOMO_TRY(configure());
-    const int Bo = std::min(batch, nYPR);
+    const int Bo = std::min(batch, n);
     const int bin_cap = 4 * P.n_tri + 4096;
     TOMO_TRY(reserve_outputs());
     TOMO_TRY(reserve_batch(Bo, bin_cap));
     TOMO_CUDA(cudaMemsetAsync(o_nbed.ptr, 0, sizeof(int) * nYPR, main));
     EngineParams p = base_params(0);
     int k = 0;
-    for (int first = 0; first < nYPR; first += Bo, k++) {
-      const int nb = std::min(Bo, nYPR - first);
+    for (int first = 0; first < n; first += Bo, k++) {
+      const int nb = std::min(Bo, n - first);
       const int which = k & 1;
       if (k >= 2) TOMO_CUDA(cudaStreamWaitEvent(main, set[which].folded, 0));
       bind_batch(p, nb, bin_cap, which, first);
+      if (ids) p.ori = ids + first;
       TOMO_CUDA(launch_batch(p, main, cfg[0].smem, &log));
       TOMO_CUDA(cudaEventRecord(ev_ready, main));
       TOMO_CUDA(cudaStreamWaitEvent(side, ev_ready, 0));
@@ -566,6 +619,13 @@ struct Engine {
   // overflows in configuration 3.
   int execute()
   {
+    if (!force_safe) TOMO_TRY(sweep_device());
+    return resolve();
+  }
+
+  // After sweep_device: fetch the results and re-run what was flagged.
+  int resolve()
+  {
     for (int& r : n_redo) r = 0;
     std::vector<int> big, safe, narrow;
     if (force_safe) {
@@ -573,7 +633,6 @@ struct Engine {
       TOMO_TRY(reserve_outputs());
       for (int i = 0; i < nYPR; i++) safe.push_back(i);
     } else {
-      TOMO_TRY(sweep_device());
       TOMO_TRY(fetch());
       for (int i = 0; i < nYPR; i++) {
         if (flags[i] & kFlagGrid) return set_error(TOMO_ERR_CAPACITY, "slot index outside the grid");
@@ -693,6 +752,61 @@ struct Engine {
     return fl;
   }
 
+  // Autotuner: times the device sweep of an evenly strided sample of up to
+  // `sample` orientations for each candidate (orientations per batch,
+  // shared-memory budget of a normal strip CTA -- which sets the strip
+  // height, the entry capacity and the CTAs per SM) and keeps the fastest.
+  // Only the speed depends on the choice: every configuration's results are
+  // exact (overflowing strips are re-run).
+  struct TuneResult { int batch, normal_smem; double us_per_orientation; };
+  int autotune(int sample, TuneResult* best)
+  {
+    static const int kBatches[] = {64, 128, 256};
+    static const int kSmem[] = {49152, 73728, 101376};
+    best->batch = batch; best->normal_smem = normal_smem; best->us_per_orientation = 0.0;
+    if (nYPR == 0 || P.n_tri == 0) return 0;
+    const int n = std::min(nYPR, std::max(sample, 1));
+    std::vector<int> ids(n);
+    for (int i = 0; i < n; i++) ids[i] = (int)((long long)i * nYPR / n);
+    DevBuf<int> dids;
+    TOMO_CUDA(dids.reserve(n));
+    TOMO_CUDA(cudaMemcpyAsync(dids.ptr, ids.data(), sizeof(int) * n, cudaMemcpyHostToDevice, main));
+    cudaEvent_t a = nullptr, b = nullptr;
+    TOMO_CUDA(cudaEventCreate(&a));
+    TOMO_CUDA(cudaEventCreate(&b));
+    const bool timing = log.timing;
+    log.timing = false;
+    const int keep_batch = batch, keep_smem = normal_smem;
+    double best_us = 1e300;
+    int rc = 0;
+    for (int bsz : kBatches) {
+      for (int sm : kSmem) {
+        batch = bsz; normal_smem = sm;
+        plan_strips();
+        float ms = 0.f;
+        // an untimed run first: it allocates and warms
+        if ((rc = sweep_device(dids.ptr, n)) != 0) break;
+        if (cudaEventRecord(a, main) != cudaSuccess) { rc = set_error(TOMO_ERR_CUDA, "autotune event"); break; }
+        if ((rc = sweep_device(dids.ptr, n)) != 0) break;
+        if (cudaEventRecord(b, main) != cudaSuccess || cudaEventSynchronize(b) != cudaSuccess ||
+            cudaEventElapsedTime(&ms, a, b) != cudaSuccess) { rc = set_error(TOMO_ERR_CUDA, "autotune timing"); break; }
+        const double us = 1000.0 * ms / n;
+        if (us < best_us) { best_us = us; best->batch = bsz; best->normal_smem = sm; }
+      }
+      if (rc) break;
+    }
+    log.timing = timing;
+    cudaStreamSynchronize(main);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    dids.release();
+    batch = rc ? keep_batch : best->batch;
+    normal_smem = rc ? keep_smem : best->normal_smem;
+    plan_strips();
+    best->us_per_orientation = best_us;
+    return rc;
+  }
+
   // Float fold of n additions of BedThickness: Calculate adds
   // sumType(typeBed) * BedThickness per bed slot (STomoSh_INT3.cpp:1240), and
   // every bed slot holds exactly one bed pixel at z = 1.
@@ -729,7 +843,7 @@ int g_npix[11] = {0};
 
 Engine& engine()
 {
-  if (!g_engine) g_engine = new Engine();
+  if (!g_engine) g_engine = new Engine(*new Workspace(), true);
   return *g_engine;
 }
 
@@ -975,7 +1089,13 @@ void OnDestroy(void)
   g_Mss.shrink_to_fit(); g_Mo.shrink_to_fit(); g_Vtc.shrink_to_fit();
   for (auto& v : g_pix) { v.clear(); v.shrink_to_fit(); }
   std::memset(g_npix, 0, sizeof(g_npix));
-  if (g_engine) { g_engine->release(); delete g_engine; g_engine = nullptr; }
+  if (g_engine) {
+    Workspace* w = &g_engine->W;
+    g_engine->release();
+    delete g_engine;
+    delete w;
+    g_engine = nullptr;
+  }
 }
 
 int tomoGetLastError(void) { return g_last_error; }
@@ -1312,7 +1432,8 @@ extern "C" int tomoSweepStatic(const float* f32info, const int* i32info, const f
       P.bed_outer > 1000.f)
     return set_error(TOMO_ERR_ARG, "bad printer parameters");
 
-  Engine X;   // strip planning and kernel parameters only; reserves nothing
+  Workspace XW;   // no streams, no buffers: strip planning and kernel parameters only
+  Engine X(XW);
   X.P = P;
   X.nYPR = P.n_ypr;
   float mn[3] = {1e5f, 1e5f, 1e5f}, mx[3] = {-1e5f, -1e5f, -1e5f};
@@ -1419,3 +1540,277 @@ extern "C" int tomoSweepStatic(const float* f32info, const int* i32info, const f
   }
   return first_optimal(P.n_ypr, Mss);
 }
+
+// ------------------------------------------------ multi-mesh batch
+//
+// Many meshes with uneven triangle counts, each with its own orientation
+// list, swept in one CUDA-graph launch: every mesh's batches (reset, rotate,
+// bin, strip, bed on the main stream; the fold on the second stream) are
+// captured once into a graph over one shared workspace and replayed with a
+// single cudaGraphLaunch.  The strip configuration (orientations per batch,
+// shared-memory budget) of each mesh is picked by Engine::autotune, once per
+// size class (slot-grid edge rounded up to 32, triangle count rounded up to
+// a power of two).  Flagged orientations are re-run per mesh afterwards by
+// the same ladder as the single-mesh call, so every mesh's results are
+// those of TomoSh_CUDA on that mesh alone.
+
+namespace tomo {
+namespace {
+
+struct MultiEngine {
+  Workspace W;
+  std::vector<Engine*> meshes;
+  std::vector<int> order;   // capture order: estimated cost, largest first
+  std::map<std::pair<int, int>, Engine::TuneResult> tuned;
+  std::vector<Engine::TuneResult> choice;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  size_t graph_nodes = 0;
+  long long graph_kernels = 0;
+  int autotune = 1;
+  int tune_sample = 512;
+  int n_tuned = 0;
+  double last_ms = 0.0;
+
+  void clear_graph()
+  {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    exec = nullptr; graph = nullptr; graph_nodes = 0; graph_kernels = 0;
+  }
+  void clear_meshes()
+  {
+    for (auto* e : meshes) { e->release(); delete e; }
+    meshes.clear(); order.clear(); choice.clear();
+  }
+  void release() { clear_graph(); clear_meshes(); W.release(); tuned.clear(); }
+
+  int prepare(int n, const float* const* f32, const int* const* i32, const float* const* ypr, const int* const* tri,
+              const float* const* vtx, const float* const* vnrm)
+  {
+    clear_graph();
+    clear_meshes();
+    TOMO_TRY(W.init());
+    for (int m = 0; m < n; m++) {
+      if (f32 == nullptr || i32 == nullptr || f32[m] == nullptr || i32[m] == nullptr)
+        return set_error(TOMO_ERR_ARG, "mesh " + std::to_string(m) + ": info arrays are null");
+      Engine* e = new Engine(W);
+      meshes.push_back(e);
+      const int rc = e->upload(f32[m], i32[m], ypr ? ypr[m] : nullptr, tri ? tri[m] : nullptr, vtx ? vtx[m] : nullptr,
+                               vnrm ? vnrm[m] : nullptr);
+      if (rc) {
+        const std::string why = g_last_error_str;
+        clear_meshes();
+        return set_error(rc, "mesh " + std::to_string(m) + ": " + why);
+      }
+    }
+    order.resize(n);
+    for (int m = 0; m < n; m++) order[m] = m;
+    auto cost = [&](int m) {
+      const Engine& e = *meshes[m];
+      return (double)e.nYPR * ((double)e.P.n_tri + 0.25 * (double)e.G * (double)e.G);
+    };
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost(a) > cost(b); });
+    choice.assign(n, Engine::TuneResult{128, 0, 0.0});
+    n_tuned = 0;
+    for (int m = 0; m < n; m++) {
+      Engine& e = *meshes[m];
+      if (!autotune || e.nYPR == 0 || e.P.n_tri == 0) { choice[m] = {e.batch, e.normal_smem, 0.0}; continue; }
+      int t = 1;
+      while (t < e.P.n_tri) t <<= 1;
+      const std::pair<int, int> key((e.G + 31) / 32 * 32, t);
+      auto it = tuned.find(key);
+      if (it == tuned.end()) {
+        Engine::TuneResult r;
+        TOMO_TRY(e.autotune(tune_sample, &r));
+        it = tuned.emplace(key, r).first;
+        n_tuned++;
+      }
+      e.batch = it->second.batch;
+      e.normal_smem = it->second.normal_smem;
+      e.plan_strips();
+      choice[m] = it->second;
+    }
+    return 0;
+  }
+
+  // Every buffer the sweep touches, at its final size, before capture.
+  int reserve_all()
+  {
+    for (auto* e : meshes) {
+      if (e->nYPR == 0 || e->P.n_tri == 0) continue;
+      e->choose_strips(0);
+      TOMO_TRY(e->configure());
+      TOMO_TRY(e->reserve_outputs());
+      TOMO_TRY(e->reserve_batch(std::min(e->batch, e->nYPR), 4 * e->P.n_tri + 4096));
+    }
+    return 0;
+  }
+
+  int capture()
+  {
+    clear_graph();
+    const bool timing = W.log.timing;
+    long long before = 0;
+    for (long long c : W.log.launches) before += c;
+    W.log.timing = false;
+    TOMO_CUDA(cudaStreamBeginCapture(W.main, cudaStreamCaptureModeThreadLocal));
+    int rc = 0;
+    for (int m : order)
+      if ((rc = meshes[m]->sweep_device()) != 0) break;
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(W.main, &g);
+    W.log.timing = timing;
+    long long after = 0;
+    for (long long c : W.log.launches) after += c;
+    graph_kernels = after - before;
+    if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+    if (e != cudaSuccess) return set_error(TOMO_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+    graph = g;
+    TOMO_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+    TOMO_CUDA(cudaGraphGetNodes(graph, nullptr, &graph_nodes));
+    return 0;
+  }
+
+  int run(int use_graph, float* device_ms)
+  {
+    if (meshes.empty()) return 0;
+    TOMO_TRY(reserve_all());
+    cudaEvent_t a = nullptr, b = nullptr;
+    TOMO_CUDA(cudaEventCreate(&a));
+    TOMO_CUDA(cudaEventCreate(&b));
+    int rc = 0;
+    if (use_graph && !exec) rc = capture();
+    if (rc == 0 && cudaEventRecord(a, W.main) != cudaSuccess) rc = set_error(TOMO_ERR_CUDA, "event record");
+    if (rc == 0) {
+      if (use_graph) {
+        const cudaError_t e = cudaGraphLaunch(exec, W.main);
+        if (e != cudaSuccess) rc = set_error(TOMO_ERR_CUDA, std::string("cudaGraphLaunch: ") + cudaGetErrorString(e));
+      } else {
+        for (int m : order)
+          if ((rc = meshes[m]->sweep_device()) != 0) break;
+      }
+    }
+    float ms = 0.f;
+    if (rc == 0) {
+      if (cudaEventRecord(b, W.main) != cudaSuccess || cudaEventSynchronize(b) != cudaSuccess ||
+          cudaEventElapsedTime(&ms, a, b) != cudaSuccess)
+        rc = set_error(TOMO_ERR_CUDA, "batch timing");
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (rc) return rc;
+    last_ms = ms;
+    if (device_ms) *device_ms = ms;
+    for (auto* e : meshes) {
+      TOMO_TRY(e->resolve());
+      e->finalize_host();
+    }
+    return 0;
+  }
+};
+
+MultiEngine* g_multi = nullptr;
+
+MultiEngine& multi()
+{
+  if (!g_multi) g_multi = new MultiEngine();
+  return *g_multi;
+}
+
+}  // namespace
+}  // namespace tomo
+
+extern "C" {
+
+int tomoBatchPrepare(int n_mesh, const float* const* f32info, const int* const* i32info, const float* const* YPR,
+                     const int* const* tri, const float* const* vtx, const float* const* vtx_nrm)
+{
+  std::lock_guard<std::mutex> lock(g_mutex);
+  g_last_error = 0; g_last_error_str.clear();
+  if (n_mesh < 0) return set_error(TOMO_ERR_ARG, "negative mesh count");
+  return multi().prepare(n_mesh, f32info, i32info, YPR, tri, vtx, vtx_nrm);
+}
+
+int tomoBatchRun(int use_graph, float* device_ms)
+{
+  std::lock_guard<std::mutex> lock(g_mutex);
+  g_last_error = 0; g_last_error_str.clear();
+  if (!g_multi) return set_error(TOMO_ERR_ARG, "tomoBatchPrepare was not called");
+  return g_multi->run(use_graph, device_ms);
+}
+
+int tomoBatchResults(int mesh, float* Mo, float* Mss, float* Vtc, long long* vo64, long long* vss64, long long* vtc64)
+{
+  std::lock_guard<std::mutex> lock(g_mutex);
+  if (!g_multi || mesh < 0 || mesh >= (int)g_multi->meshes.size()) return set_error(TOMO_ERR_ARG, "bad mesh index");
+  const Engine& E = *g_multi->meshes[mesh];
+  const size_t n = (size_t)E.nYPR;
+  if (E.Mss.size() < n) return set_error(TOMO_ERR_ARG, "tomoBatchRun was not called");
+  if (Mo) std::memcpy(Mo, E.Mo.data(), sizeof(float) * n);
+  if (Mss) std::memcpy(Mss, E.Mss.data(), sizeof(float) * n);
+  if (Vtc) std::memcpy(Vtc, E.Vtc.data(), sizeof(float) * n);
+  if (vo64 && E.vo64.size() >= n) std::memcpy(vo64, E.vo64.data(), sizeof(long long) * n);
+  if (vss64 && E.vss64.size() >= n) std::memcpy(vss64, E.vss64.data(), sizeof(long long) * n);
+  if (vtc64 && E.vtc64.size() >= n) std::memcpy(vtc64, E.vtc64.data(), sizeof(long long) * n);
+  return first_optimal((int)n, E.Mss.data());
+}
+
+int tomoBatchStats(long long* out, int n)
+{
+  std::lock_guard<std::mutex> lock(g_mutex);
+  if (!g_multi || out == nullptr) return TOMO_ERR_ARG;
+  const MultiEngine& M = *g_multi;
+  long long orient = 0, redo = 0;
+  for (auto* e : M.meshes) { orient += e->nYPR; redo += e->n_redo[1] + e->n_redo[2] + e->n_redo[3]; }
+  const long long v[8] = {(long long)M.meshes.size(), orient, (long long)M.graph_nodes, M.graph_kernels,
+                          (long long)M.n_tuned, (long long)M.tuned.size(), redo, (long long)(M.last_ms * 1000.0)};
+  for (int k = 0; k < n && k < 8; k++) out[k] = v[k];
+  return 0;
+}
+
+int tomoBatchConfig(int mesh, int* out4)
+{
+  std::lock_guard<std::mutex> lock(g_mutex);
+  if (!g_multi || mesh < 0 || mesh >= (int)g_multi->meshes.size() || out4 == nullptr)
+    return set_error(TOMO_ERR_ARG, "bad mesh index");
+  const Engine& E = *g_multi->meshes[mesh];
+  out4[0] = E.batch;
+  out4[1] = E.normal_smem;
+  out4[2] = E.cfg[0].H;
+  out4[3] = E.G;
+  return 0;
+}
+
+int TomoSh_CUDA_Batch(int n_mesh, const float* const* f32info, const int* const* i32info, const float* const* YPR,
+                      const int* const* tri, const float* const* vtx, const float* const* vtx_nrm, int* optIDs)
+{
+  int rc = tomoBatchPrepare(n_mesh, f32info, i32info, YPR, tri, vtx, vtx_nrm);
+  if (rc) return rc;
+  rc = tomoBatchRun(1, nullptr);
+  if (rc) return rc;
+  for (int m = 0; m < n_mesh; m++) {
+    const int o = tomoBatchResults(m, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr);
+    if (o < 0) return o;
+    if (optIDs) optIDs[m] = o;
+  }
+  return 0;
+}
+
+void tomoBatchRelease(void)
+{
+  std::lock_guard<std::mutex> lock(g_mutex);
+  if (g_multi) { g_multi->release(); delete g_multi; g_multi = nullptr; }
+}
+
+int tomoBatchSetOption(int key, int value)
+{
+  std::lock_guard<std::mutex> lock(g_mutex);
+  switch (key) {
+    case 1: multi().autotune = value ? 1 : 0; return 0;
+    case 2: if (value < 1) return TOMO_ERR_ARG; multi().tune_sample = value; return 0;
+    default: return TOMO_ERR_ARG;
+  }
+}
+
+}  // extern "C"

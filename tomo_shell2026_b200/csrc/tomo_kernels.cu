@@ -1242,11 +1242,27 @@ size_t strip_smem_bytes(int mode, int H, int G, int ent_cap)
   return strip_smem_layout(mode, H, G, ent_cap);
 }
 
+// The strip kernels' dynamic shared-memory limit only ever rises (per
+// device), so every caller's launches stay within it and the attribute is
+// set only when a larger configuration first appears.
 cudaError_t configure_kernels(size_t normal_smem, size_t safe_smem)
 {
-  cudaError_t e = cudaFuncSetAttribute(k_strip<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)normal_smem);
+  static size_t conf[64][2];
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(k_strip<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)safe_smem);
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  if (normal_smem > conf[dev][0]) {
+    e = cudaFuncSetAttribute(k_strip<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)normal_smem);
+    if (e != cudaSuccess) return e;
+    conf[dev][0] = normal_smem;
+  }
+  if (safe_smem > conf[dev][1]) {
+    e = cudaFuncSetAttribute(k_strip<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)safe_smem);
+    if (e != cudaSuccess) return e;
+    conf[dev][1] = safe_smem;
+  }
+  return cudaSuccess;
 }
 
 // Launch bookkeeping: every launch is counted; with timing on, a pair of

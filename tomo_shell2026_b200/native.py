@@ -55,6 +55,14 @@ EXPORTS = [
     ("tomoGetKernelLog", ct.c_int, [_i64p, ct.POINTER(ct.c_double), _i64p, ct.c_int]),
     ("tomoColumnDump", ct.c_int, [ct.c_int, ct.c_int, _i32p, _u32p, _i16p]),
     ("tomoSweepStatic", ct.c_int, [_f32p, _i32p, _f32p, _i32p, _f32p, _f32p, _f32p, _f32p, _f32p, ct.c_void_p]),
+    ("tomoBatchPrepare", ct.c_int, [ct.c_int] + [ct.POINTER(ct.c_void_p)] * 6),
+    ("tomoBatchRun", ct.c_int, [ct.c_int, _f32p]),
+    ("tomoBatchResults", ct.c_int, [ct.c_int, _f32p, _f32p, _f32p, _i64p, _i64p, _i64p]),
+    ("TomoSh_CUDA_Batch", ct.c_int, [ct.c_int] + [ct.POINTER(ct.c_void_p)] * 6 + [_i32p]),
+    ("tomoBatchStats", ct.c_int, [_i64p, ct.c_int]),
+    ("tomoBatchConfig", ct.c_int, [ct.c_int, _i32p]),
+    ("tomoBatchSetOption", ct.c_int, [ct.c_int, ct.c_int]),
+    ("tomoBatchRelease", None, []),
 ]
 
 _LIB: ct.CDLL | None = None
@@ -209,6 +217,62 @@ def sweep(mesh, ypr, opts) -> SweepResult:
                        r["VoF"], r["VssF"], r["VtcF"], r["n_bed"], r["flags"], r["entries"], r["columns"],
                        np.ctypeslib.as_array(L.getVolMassInfo(), shape=(22,)).copy(),
                        np.ctypeslib.as_array(L.getMat4x4(), shape=(16,)).copy().reshape(4, 4), pixels())
+
+
+class Batch:
+    """Many meshes, one graph launch (tomoBatchPrepare / tomoBatchRun)."""
+
+    def __init__(self, meshes, yprs, opts, autotune: bool = True, tune_sample: int = 512):
+        from .options import pack_info
+        if not isinstance(opts, (list, tuple)):
+            opts = [opts] * len(meshes)
+        self.n = [int(y.shape[0]) for y in yprs]
+        self._keep = []
+        cols = [[] for _ in range(6)]
+        for m, y, o in zip(meshes, yprs, opts):
+            f32, i32 = pack_info(o, m, y.shape[0])
+            y, tri, vtx, vn, *_ = _arrays(m, y)
+            self._keep += [f32, i32, y, tri, vtx, vn]
+            for c, a in zip(cols, (f32, i32, y, tri, vtx, vn)):
+                c.append(a.ctypes.data)
+        self._ptrs = [(ct.c_void_p * max(len(meshes), 1))(*c) for c in cols]
+        L = lib()
+        _check(L.tomoBatchSetOption(1, 1 if autotune else 0))
+        _check(L.tomoBatchSetOption(2, int(tune_sample)))
+        _check(L.tomoBatchPrepare(len(meshes), *self.pointer_args()))
+
+    def pointer_args(self):
+        return [ct.cast(p, ct.POINTER(ct.c_void_p)) for p in self._ptrs]
+
+    def run(self, use_graph: bool = True) -> float:
+        ms = ct.c_float(0.0)
+        _check(lib().tomoBatchRun(1 if use_graph else 0, ct.byref(ms)))
+        return float(ms.value)
+
+    def results(self, m: int) -> dict:
+        n = self.n[m]
+        out = {k: np.zeros(n, np.float32) for k in ("Mo", "Mss", "Vtc")}
+        out.update({k: np.zeros(n, np.int64) for k in ("Vo64", "Vss64", "Vtc64")})
+        out["optID"] = _check(lib().tomoBatchResults(m, *[_p(out[k], _f32p) for k in ("Mo", "Mss", "Vtc")],
+                                                       *[_p(out[k], _i64p) for k in ("Vo64", "Vss64", "Vtc64")]))
+        return out
+
+    def config(self, m: int) -> dict:
+        c = np.zeros(4, np.int32)
+        _check(lib().tomoBatchConfig(m, _p(c, _i32p)))
+        return dict(batch=int(c[0]), normal_smem=int(c[1]), strip_h=int(c[2]), grid=int(c[3]))
+
+    @staticmethod
+    def stats() -> dict:
+        out = np.zeros(8, np.int64)
+        _check(lib().tomoBatchStats(_p(out, _i64p), 8))
+        keys = ("meshes", "orientations", "graph_nodes", "graph_kernels", "tuned_now", "tuned_total", "reruns",
+                "device_us")
+        return {k: int(v) for k, v in zip(keys, out)}
+
+    @staticmethod
+    def release() -> None:
+        lib().tomoBatchRelease()
 
 
 def sweep_static(mesh, ypr, opts, stream: int | None = None) -> tuple[int, np.ndarray, np.ndarray, np.ndarray]:
