@@ -30,7 +30,7 @@ extern "C" {
 /* ---- reference-compatible exports ---------------------------------------- */
 
 /* Exhaustive orientation search.  Replaces TomoSh_CUDA / TomoSh_INT3
- * (Tomo_Shell2026.h:33-35, Tomo_Shell2026.cpp:296-299,367-417).
+ * (Tomo_Shell2026.h:33-35, Tomo_Shell2026.cpp:119-248,257-260,328-378).
  *   f32info[12]  dVoxel, theta_c, surface_area, wall_thickness, Fcore, Fclad,
  *                Fss, Css, PLA_density, BedInnerBound, BedOuterBound, BedThickness
  *                (S3DPrinterInfo.h:42-47)
@@ -41,12 +41,12 @@ extern "C" {
  *                hull arrays are accepted and unused (the INT3 arithmetic does
  *                not read them).
  * Returns optID = first index of the strictly smallest Mss starting from
- * 1e5 (_find1stOptimal, Tomo_Shell2026.cpp:128-136), or a negative error. */
+ * 1e5 (_find1stOptimal, Tomo_Shell2026.cpp:89-97), or a negative error. */
 int TomoSh_CUDA(float* f32info, int* i32info, float* YPR, int* tri, float* vtx, float* vtx_nrm, float* tri_nrm,
                 int* chull_tri, float* chull_vtx, float* chull_trinrm);
 
 /* Same call under the reference's CPU-engine name (Tomo_Shell2026.h:33,
- * Tomo_Shell2026.cpp:296-299): the reference INT3 results, computed on the GPU. */
+ * Tomo_Shell2026.cpp:257-260): the reference INT3 results, computed on the GPU. */
 int TomoSh_INT3(float* f32info, int* i32info, float* YPR, int* tri, float* vtx, float* vtx_nrm, float* tri_nrm,
                 int* chull_tri, float* chull_vtx, float* chull_trinrm);
 

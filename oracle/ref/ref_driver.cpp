@@ -5,7 +5,7 @@
 // oracle/_ref/libtomo_ref.so.  It is the reference itself, driven from C:
 // the per-orientation step sequence, the thread fan-out and the argmin follow
 // _TomoSh_Function_Call / thread_func / _find1stOptimal
-// (cfms_tomo/Tomo_Shell_vc_src/Tomo_Shell2026.cpp:128-288).  Two additions,
+// (cfms_tomo/Tomo_Shell_vc_src/Tomo_Shell2026.cpp:89-248).  Two additions,
 // both read-only with respect to the engine's arithmetic:
 //
 //   * exact int64 per-orientation totals of the per-column Vo/Vss, summed
@@ -65,7 +65,7 @@ struct SweepOut {
   long long* Vo64; long long* Vss64; long long* Vtc64;
 };
 
-// thread_func (Tomo_Shell2026.cpp:138-156) plus the int64 side channel.
+// thread_func (Tomo_Shell2026.cpp:99-117) plus the int64 side channel.
 void runOne(STomoSh_INT3* nv, const float* ypr, int id, const SweepOut& o)
 {
   S3DPrinterInfo& info = nv->printer_info;
@@ -100,7 +100,7 @@ void runOne(STomoSh_INT3* nv, const float* ypr, int id, const SweepOut& o)
   o.Vtc[id] = nv->vm_info.Vtc;
 }
 
-// _find1stOptimal (Tomo_Shell2026.cpp:128-136).
+// _find1stOptimal (Tomo_Shell2026.cpp:89-97).
 int firstOptimal(int n, const float* mss)
 {
   if (n <= 1) return 0;
@@ -125,7 +125,7 @@ void prepare(STomoSh_INT3* pNV, int n, const S3DPrinterInfo& info, int grid)
 extern "C" {
 
 // Full orientation sweep through the reference INT3 engine.  Orchestration
-// follows _TomoSh_Function_Call (Tomo_Shell2026.cpp:194-258): blocks of
+// follows _TomoSh_Function_Call (Tomo_Shell2026.cpp:194-215): blocks of
 // n_threads std::threads, one orientation each, joined per block.  Returns
 // the reference optID.  Vo64/Vss64/Vtc64/VoF/VssF may be null.
 int ref_int3_sweep(const float* f32info, const int* i32info, const float* ypr,

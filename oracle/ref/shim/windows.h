@@ -9,7 +9,7 @@
  * The reference reaches <windows.h> through pch.h -> framework.h
  * (cfms_tomo/Tomo_Shell_vc_src/framework.h:5) and uses only three things
  * from the Win32 / MSVC CRT world:
- *   - _dupenv_s  (debug env switches, e.g. STomoSh_INT3.cpp:23, Tomo_Shell2026.cpp:202)
+ *   - _dupenv_s  (debug env switches, e.g. STomoSh_INT3.cpp:23, Tomo_Shell2026.cpp:145,163)
  *   - fopen_s    (debug CSV dumps, e.g. STomoSh_INT3.cpp:92)
  *   - the min/max function-like macros windows.h defines without NOMINMAX
  *     (STomoSh_INT3.cpp:560,1344,1346,1359,1403,1404)

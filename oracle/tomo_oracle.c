@@ -653,7 +653,7 @@ static void* sweep_worker(void* arg)
   return NULL;
 }
 
-/* _find1stOptimal (Tomo_Shell2026.cpp:128-136) */
+/* _find1stOptimal (Tomo_Shell2026.cpp:89-97) */
 static int first_optimal(int n, const float* mss)
 {
   if (n <= 1) return 0;

@@ -32,7 +32,7 @@ float tomo_oracle_threshold(float theta_c);
 void tomo_oracle_vol_to_mass(const float* f32info12, const int32_t* i32info11, float* vm22);
 
 /* Whole sweep.  Returns the reference optID (_find1stOptimal,
- * Tomo_Shell2026.cpp:128-136) or a negative error code:
+ * Tomo_Shell2026.cpp:89-97) or a negative error code:
  *   -1 bad arguments, -2 out of memory, -3 a slot index fell outside the grid.
  * grid: square slot grid edge (0 = 256, the reference default).
  * Outputs are [nYPR] and may be NULL. */

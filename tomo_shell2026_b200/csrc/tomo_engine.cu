@@ -137,7 +137,7 @@ void vol_to_mass(const Params& P, float* vm)
   vm[19] = Mo + Mss;
 }
 
-// _find1stOptimal (Tomo_Shell2026.cpp:128-136)
+// _find1stOptimal (Tomo_Shell2026.cpp:89-97)
 int first_optimal(int n, const float* mss)
 {
   if (n <= 1) return 0;

@@ -3,7 +3,7 @@
 Orientations are independent, so a sweep partitions into contiguous shards
 of the YPR array with no exchange on the data path.  The one cross-rank
 step is the final argmin, which must reproduce _find1stOptimal
-(Tomo_Shell_vc_src/Tomo_Shell2026.cpp:128-136): the first index whose Mss is
+(Tomo_Shell_vc_src/Tomo_Shell2026.cpp:89-97): the first index whose Mss is
 strictly below the running minimum, the running minimum starting at 1e5
 (result 0 when nothing is below 1e5, or when there is at most one
 orientation).  Each rank reduces its shard to (first minimal Mss, global
@@ -46,7 +46,7 @@ def local_candidate(mss_shard: np.ndarray, begin: int) -> int:
 
 
 def first_optimal(mss: np.ndarray) -> int:
-    """_find1stOptimal on one array (Tomo_Shell2026.cpp:128-136)."""
+    """_find1stOptimal on one array (Tomo_Shell2026.cpp:89-97)."""
     if len(mss) <= 1:
         return 0
     key = local_candidate(mss, 0)
