@@ -161,6 +161,44 @@ int tomoBatchConfig(int mesh, int* out4);
 int tomoBatchSetOption(int key, int value);
 void tomoBatchRelease(void);
 
+/* ---- learned-proposal search (no reference counterpart) -------------------
+ * The surrogate network: an FP32 MLP [sin yaw, cos yaw, sin pitch, cos pitch]
+ * -> 128 -> 128 -> 128 -> 1 (tanh hidden units, linear output) trained with
+ * mean squared error and Adam by the library's own CUDA kernels.  Host
+ * arrays: x[n][4] features, y[n] targets.  Parameters are one flat float
+ * vector (per layer weights [in][out] row-major, then biases; 33,793 in all).
+ *   tomoMlpInit      seeded initialisation, Adam state cleared; returns the parameter count
+ *   tomoMlpParams    copy the parameters out (get) and/or in (set; clears Adam state)
+ *   tomoMlpGrad      forward + backward on (x, y): flat gradient and loss
+ *   tomoMlpAdam      one Adam step from the last gradient
+ *   tomoMlpFit       steps x (gradient + Adam) on (x, y); loss of the last step
+ *   tomoMlpPredict   out[n] = network(x) */
+int tomoMlpInit(int seed);
+int tomoMlpParams(float* get, const float* set);
+int tomoMlpGrad(const float* x, const float* y, int n, float* grad, float* loss);
+int tomoMlpAdam(float lr);
+int tomoMlpFit(const float* x, const float* y, int n, int steps, float lr, float* loss);
+int tomoMlpPredict(const float* x, int n, float* out);
+
+/* Learned-proposal search over a YPR grid laid out [n_pitch][n_yaw] (yaw
+ * fastest; n_yaw * n_pitch = Int32Info[6]): the exact kernels evaluate the
+ * coarse points (both indices multiples of `cell`), the network is trained on
+ * their exact Vss, ranks the cell x cell blocks by predicted Vss, the top_k
+ * blocks are evaluated exactly, then every block whose smallest prediction is
+ * within the largest observed out-of-sample error of the best exact Vss, round
+ * after round; more than max_expand extra blocks, a mean relative error above
+ * `gate`, or a bed (Mss then not monotone in Vss) fall back to the exhaustive
+ * sweep.  iparams = {cell, top_k, train_steps, seed, max_expand},
+ * fparams = {learning_rate, gate}.  Returns optID (_find1stOptimal over the
+ * evaluated orientations, grid order).  Mss_out[nYPR]: exact Mss where
+ * evaluated, NaN elsewhere; pred_out[nYPR]: predicted Vss (either may be
+ * null).  stats[12] = evaluated orientations, fell back (0/1), mean relative
+ * error, max abs error, final training loss, seconds total / exact sweeps /
+ * training / prediction, blocks refined, expansion rounds, coarse points. */
+int tomoSurrogateSearch(const float* f32info, const int* i32info, const float* YPR, const int* tri, const float* vtx,
+                        const float* vtx_nrm, int n_yaw, int n_pitch, const int* iparams, const float* fparams,
+                        float* Mss_out, float* pred_out, double* stats);
+
 /* Allocation-free form of TomoSh_CUDA for small meshes.  No counterpart in the
  * reference.  Same inputs as TomoSh_CUDA; Mo, Mss and Vtc are caller-owned
  * host arrays of nYPR floats that receive what getMo/getMss/getVtc return

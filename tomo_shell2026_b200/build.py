@@ -21,8 +21,8 @@ LIB = OUT_DIR / "libtomo_b200.so"
 INCLUDE = PKG.parent / "include"
 NVCC = os.environ.get("NVCC", str(Path(os.environ.get("CUDA_HOME", "/usr/local/cuda")) / "bin" / "nvcc"))
 
-SOURCES = ["tomo_kernels.cu", "tomo_engine.cu"]
-HEADERS = ["tomo_common.cuh"]
+SOURCES = ["tomo_kernels.cu", "tomo_engine.cu", "tomo_mlp.cu"]
+HEADERS = ["tomo_common.cuh", "tomo_mlp.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

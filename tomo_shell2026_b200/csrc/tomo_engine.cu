@@ -12,9 +12,11 @@
 // floats are bit-identical by construction; everything per vertex, triangle,
 // pixel and column runs in the kernels of tomo_kernels.cu.
 #include "tomo_common.cuh"
+#include "tomo_mlp.cuh"
 #include "../../include/tomo_b200.h"
 
 #include <algorithm>
+#include <chrono>
 #include <climits>
 #include <cmath>
 #include <cstdio>
@@ -34,6 +36,7 @@ cudaError_t launch_fold(const EngineParams& p, cudaStream_t side, LaunchLog* L);
 cudaError_t launch_bin_count(const EngineParams& p, cudaStream_t main, LaunchLog* L);
 cudaError_t launch_after_count(const EngineParams& p, cudaStream_t main, size_t strip_smem, LaunchLog* L);
 cudaError_t launch_dump_scan(const int* cols8, int GG, int* off, int* totals, cudaStream_t s);
+cudaError_t launch_zero_ids(int* out, const int* ids, int n, cudaStream_t s);
 cudaError_t launch_dump_gather(const int* cols8, const unsigned* keys64, const short* types64, int GG, const int* off,
                                int* cols9, unsigned* keys, short* types, cudaStream_t s);
 
@@ -524,7 +527,8 @@ struct Engine {
     const int bin_cap = 4 * P.n_tri + 4096;
     TOMO_TRY(reserve_outputs());
     TOMO_TRY(reserve_batch(Bo, bin_cap));
-    TOMO_CUDA(cudaMemsetAsync(o_nbed.ptr, 0, sizeof(int) * nYPR, main));
+    if (ids) TOMO_CUDA(launch_zero_ids(o_nbed.ptr, ids, n, main));
+    else TOMO_CUDA(cudaMemsetAsync(o_nbed.ptr, 0, sizeof(int) * nYPR, main));
     EngineParams p = base_params(0);
     int k = 0;
     for (int first = 0; first < n; first += Bo, k++) {
@@ -624,17 +628,24 @@ struct Engine {
   }
 
   // After sweep_device: fetch the results and re-run what was flagged.
-  int resolve()
+  // With `subset`, only those orientations were swept and are checked.
+  int resolve(const std::vector<int>* subset = nullptr)
   {
     for (int& r : n_redo) r = 0;
+    std::vector<int> all;
+    if (!subset) {
+      all.resize(nYPR);
+      for (int i = 0; i < nYPR; i++) all[i] = i;
+      subset = &all;
+    }
     std::vector<int> big, safe, narrow;
     if (force_safe) {
       if (nYPR == 0 || P.n_tri == 0) return fetch();
       TOMO_TRY(reserve_outputs());
-      for (int i = 0; i < nYPR; i++) safe.push_back(i);
+      safe = *subset;
     } else {
       TOMO_TRY(fetch());
-      for (int i = 0; i < nYPR; i++) {
+      for (int i : *subset) {
         if (flags[i] & kFlagGrid) return set_error(TOMO_ERR_CAPACITY, "slot index outside the grid");
         if (flags[i] & (kFlagStray | kFlagBinCap)) safe.push_back(i);
         else if (flags[i] & kFlagOverflow) big.push_back(i);
@@ -656,7 +667,7 @@ struct Engine {
       TOMO_TRY(run_subset(narrow, 3));
       TOMO_TRY(fetch());
     }
-    for (int i = 0; i < nYPR; i++) {
+    for (int i : *subset) {
       if (flags[i] & kFlagSafeOverflow) return set_error(TOMO_ERR_CAPACITY, "column strip exceeds shared memory");
       if (flags[i] & kFlagGrid) return set_error(TOMO_ERR_CAPACITY, "slot index outside the grid");
       if (flags[i] & (kFlagStray | kFlagOverflow | kFlagBinCap))
@@ -1811,6 +1822,280 @@ int tomoBatchSetOption(int key, int value)
     case 2: if (value < 1) return TOMO_ERR_ARG; multi().tune_sample = value; return 0;
     default: return TOMO_ERR_ARG;
   }
+}
+
+}  // extern "C"
+
+// ------------------------------------------------ learned-proposal search
+//
+// The orientation grid is YPR[n_pitch][n_yaw] (yaw fastest), cut into cells
+// of cell x cell grid points.  The exact kernels evaluate the coarse points
+// (both grid indices multiples of `cell`); the MLP of tomo_mlp.cu is trained
+// on their exact Vss (standardised) from [sin y, cos y, sin p, cos p],
+// predicts Vss on every grid point, and the cells are ranked by their
+// smallest prediction.  The top_k cells are evaluated exactly.  The largest
+// prediction error seen on those out-of-sample points, err, then decides
+// which other cells could still hold something better than the best exact
+// Vss found: every cell whose smallest prediction is within err of it is
+// evaluated too, round after round.  If that would take more than
+// max_expand cells, or the mean relative error on the refined points
+// exceeds `gate`, the search falls back to the exhaustive sweep.  With the
+// bed off, Mss is a non-decreasing function of Vss (VolToMass), so ranking
+// by Vss ranks by Mss; with a bed the search always falls back.  The answer
+// is _find1stOptimal over the evaluated orientations in grid order.
+
+namespace tomo {
+namespace {
+
+Mlp* g_mlp = nullptr;
+
+Mlp& mlp()
+{
+  if (!g_mlp) g_mlp = new Mlp();
+  return *g_mlp;
+}
+
+double seconds_since(std::chrono::steady_clock::time_point t0)
+{
+  return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+// Exact evaluation of `ids` on the device (configuration 0 plus the re-run ladder).
+int eval_ids(Engine& E, const std::vector<int>& ids, DevBuf<int>& dids)
+{
+  if (ids.empty()) return 0;
+  TOMO_CUDA(dids.reserve(ids.size()));
+  TOMO_CUDA(cudaMemcpyAsync(dids.ptr, ids.data(), sizeof(int) * ids.size(), cudaMemcpyHostToDevice, E.main));
+  TOMO_TRY(E.sweep_device(dids.ptr, (int)ids.size()));
+  TOMO_TRY(E.resolve(&ids));
+  return 0;
+}
+
+}  // namespace
+}  // namespace tomo
+
+extern "C" {
+
+int tomoMlpInit(int seed)
+{
+  std::lock_guard<std::mutex> lock(g_mutex);
+  Engine& E = engine();
+  TOMO_TRY(E.init());
+  TOMO_CUDA(mlp().init((unsigned)seed, E.main));
+  return mlp().param_count();
+}
+
+int tomoMlpParams(float* get, const float* set)
+{
+  std::lock_guard<std::mutex> lock(g_mutex);
+  if (!g_mlp) return set_error(TOMO_ERR_ARG, "tomoMlpInit was not called");
+  Engine& E = engine();
+  if (set) TOMO_CUDA(mlp().set_params(set, E.main));
+  if (get) TOMO_CUDA(mlp().get_params(get, E.main));
+  return mlp().param_count();
+}
+
+int tomoMlpGrad(const float* x, const float* y, int n, float* grad, float* loss)
+{
+  std::lock_guard<std::mutex> lock(g_mutex);
+  if (!g_mlp) return set_error(TOMO_ERR_ARG, "tomoMlpInit was not called");
+  if (n <= 0 || x == nullptr || y == nullptr) return set_error(TOMO_ERR_ARG, "empty training data");
+  Engine& E = engine();
+  TOMO_CUDA(mlp().set_data(x, y, n, E.main));
+  TOMO_CUDA(mlp().grad(E.main));
+  TOMO_CUDA(mlp().read_grad(grad, loss, E.main));
+  return 0;
+}
+
+int tomoMlpAdam(float lr)
+{
+  std::lock_guard<std::mutex> lock(g_mutex);
+  if (!g_mlp) return set_error(TOMO_ERR_ARG, "tomoMlpInit was not called");
+  Engine& E = engine();
+  TOMO_CUDA(mlp().adam(lr, E.main));
+  TOMO_CUDA(cudaStreamSynchronize(E.main));
+  return 0;
+}
+
+int tomoMlpFit(const float* x, const float* y, int n, int steps, float lr, float* loss)
+{
+  std::lock_guard<std::mutex> lock(g_mutex);
+  if (!g_mlp) return set_error(TOMO_ERR_ARG, "tomoMlpInit was not called");
+  if (n <= 0 || x == nullptr || y == nullptr || steps < 0) return set_error(TOMO_ERR_ARG, "bad training arguments");
+  Engine& E = engine();
+  TOMO_CUDA(mlp().set_data(x, y, n, E.main));
+  TOMO_CUDA(mlp().fit(steps, lr, E.main, loss));
+  return 0;
+}
+
+int tomoMlpPredict(const float* x, int n, float* out)
+{
+  std::lock_guard<std::mutex> lock(g_mutex);
+  if (!g_mlp) return set_error(TOMO_ERR_ARG, "tomoMlpInit was not called");
+  if (n <= 0 || x == nullptr || out == nullptr) return set_error(TOMO_ERR_ARG, "bad prediction arguments");
+  Engine& E = engine();
+  DevBuf<float> dx, dy;
+  TOMO_CUDA(dx.reserve((size_t)n * kMlpIn));
+  TOMO_CUDA(dy.reserve((size_t)n));
+  TOMO_CUDA(cudaMemcpyAsync(dx.ptr, x, sizeof(float) * n * kMlpIn, cudaMemcpyHostToDevice, E.main));
+  TOMO_CUDA(mlp().predict_device(dx.ptr, n, dy.ptr, E.main));
+  TOMO_CUDA(cudaMemcpyAsync(out, dy.ptr, sizeof(float) * n, cudaMemcpyDeviceToHost, E.main));
+  TOMO_CUDA(cudaStreamSynchronize(E.main));
+  dx.release();
+  dy.release();
+  return 0;
+}
+
+int tomoSurrogateSearch(const float* f32info, const int* i32info, const float* YPR, const int* tri, const float* vtx,
+                        const float* vtx_nrm, int n_yaw, int n_pitch, const int* iparams, const float* fparams,
+                        float* Mss_out, float* pred_out, double* stats)
+{
+  std::lock_guard<std::mutex> lock(g_mutex);
+  g_last_error = 0; g_last_error_str.clear();
+  const auto t_start = std::chrono::steady_clock::now();
+  if (f32info == nullptr || i32info == nullptr || iparams == nullptr || fparams == nullptr)
+    return set_error(TOMO_ERR_ARG, "null argument");
+  const int cell = iparams[0], top_k = iparams[1], steps = iparams[2], seed = iparams[3], max_expand = iparams[4];
+  const float lr = fparams[0], gate = fparams[1];
+  if (n_yaw <= 0 || n_pitch <= 0 || (long long)n_yaw * n_pitch != i32info[6])
+    return set_error(TOMO_ERR_ARG, "n_yaw * n_pitch must equal nYPR");
+  if (cell < 1 || top_k < 1 || steps < 0 || max_expand < 0) return set_error(TOMO_ERR_ARG, "bad search parameters");
+  Engine& E = engine();
+  TOMO_TRY(E.init());
+  TOMO_TRY(E.upload(f32info, i32info, YPR, tri, vtx, vtx_nrm));
+  const int n = E.nYPR;
+  double t_exact = 0.0, t_train = 0.0, t_pred = 0.0;
+  std::vector<char> done(n, 0);
+  std::vector<int> evaluated;
+  DevBuf<int> dids;
+  auto evaluate = [&](const std::vector<int>& ids) -> int {
+    const auto t0 = std::chrono::steady_clock::now();
+    const int rc = eval_ids(E, ids, dids);
+    t_exact += seconds_since(t0);
+    if (rc) return rc;
+    for (int i : ids) { done[i] = 1; evaluated.push_back(i); }
+    return 0;
+  };
+  const int ncy = (n_yaw + cell - 1) / cell, ncp = (n_pitch + cell - 1) / cell, ncell = ncy * ncp;
+  auto cell_of = [&](int id) { return (id % n_yaw) / cell + ((id / n_yaw) / cell) * ncy; };
+  std::vector<float> pred(n, 0.f);
+  double rel_err = 0.0, max_err = 0.0;
+  float train_loss = 0.f;
+  int fallback = 0, rounds = 0, cells_refined = 0, n_coarse = 0;
+
+  if (E.P.bed_type != kBedNone || E.P.n_tri == 0) {
+    fallback = 1;
+  } else {
+    // 1. coarse points, exact
+    std::vector<int> coarse;
+    for (int ip = 0; ip < n_pitch; ip += cell)
+      for (int iy = 0; iy < n_yaw; iy += cell) coarse.push_back(ip * n_yaw + iy);
+    n_coarse = (int)coarse.size();
+    TOMO_TRY(evaluate(coarse));
+    // 2. train on standardised exact Vss
+    auto feat = [&](int id, float* f) {
+      const float y = YPR[id * 3 + 0], p = YPR[id * 3 + 1];
+      f[0] = sinf(y); f[1] = cosf(y); f[2] = sinf(p); f[3] = cosf(p);
+    };
+    double mean = 0.0, sq = 0.0;
+    for (int id : coarse) mean += (double)E.vss64[id];
+    mean /= (double)coarse.size();
+    for (int id : coarse) sq += ((double)E.vss64[id] - mean) * ((double)E.vss64[id] - mean);
+    const double sd = coarse.size() > 1 && sq > 0.0 ? std::sqrt(sq / (double)coarse.size()) : 1.0;
+    std::vector<float> X(coarse.size() * kMlpIn), Y(coarse.size());
+    for (size_t k = 0; k < coarse.size(); k++) {
+      feat(coarse[k], &X[k * kMlpIn]);
+      Y[k] = (float)(((double)E.vss64[coarse[k]] - mean) / sd);
+    }
+    {
+      const auto t0 = std::chrono::steady_clock::now();
+      TOMO_CUDA(mlp().init((unsigned)seed, E.main));
+      TOMO_CUDA(mlp().set_data(X.data(), Y.data(), (int)coarse.size(), E.main));
+      TOMO_CUDA(mlp().fit(steps, lr, E.main, &train_loss));
+      t_train += seconds_since(t0);
+    }
+    // 3. predict every grid point
+    {
+      const auto t0 = std::chrono::steady_clock::now();
+      std::vector<float> F((size_t)n * kMlpIn);
+      for (int id = 0; id < n; id++) feat(id, &F[(size_t)id * kMlpIn]);
+      DevBuf<float> dx, dy;
+      TOMO_CUDA(dx.reserve(F.size()));
+      TOMO_CUDA(dy.reserve((size_t)n));
+      TOMO_CUDA(cudaMemcpyAsync(dx.ptr, F.data(), sizeof(float) * F.size(), cudaMemcpyHostToDevice, E.main));
+      TOMO_CUDA(mlp().predict_device(dx.ptr, n, dy.ptr, E.main));
+      TOMO_CUDA(cudaMemcpyAsync(pred.data(), dy.ptr, sizeof(float) * n, cudaMemcpyDeviceToHost, E.main));
+      TOMO_CUDA(cudaStreamSynchronize(E.main));
+      dx.release();
+      dy.release();
+      for (int id = 0; id < n; id++) pred[id] = (float)(pred[id] * sd + mean);
+      t_pred += seconds_since(t0);
+    }
+    // 4. cells by smallest prediction; refine the top_k
+    std::vector<float> cmin(ncell, INFINITY);
+    for (int id = 0; id < n; id++) { const int c = cell_of(id); cmin[c] = std::min(cmin[c], pred[id]); }
+    std::vector<int> rank(ncell);
+    for (int c = 0; c < ncell; c++) rank[c] = c;
+    std::stable_sort(rank.begin(), rank.end(), [&](int a, int b) { return cmin[a] < cmin[b]; });
+    std::vector<char> refined(ncell, 0);
+    auto refine_cells = [&](const std::vector<int>& cells) -> int {
+      std::vector<int> ids;
+      for (int c : cells) refined[c] = 1;
+      for (int id = 0; id < n; id++)
+        if (!done[id] && refined[cell_of(id)]) ids.push_back(id);
+      cells_refined += (int)cells.size();
+      return evaluate(ids);
+    };
+    std::vector<int> first(rank.begin(), rank.begin() + std::min(top_k, ncell));
+    TOMO_TRY(refine_cells(first));
+    // 5. error gate and expansion
+    for (;; rounds++) {
+      double sum_abs = 0.0, sum_ref = 0.0;
+      max_err = 0.0;
+      long long best = LLONG_MAX;
+      int m = 0;
+      for (int id : evaluated) {
+        best = std::min(best, E.vss64[id]);
+        if ((id % n_yaw) % cell == 0 && (id / n_yaw) % cell == 0) continue;   // training point
+        const double e = std::fabs((double)pred[id] - (double)E.vss64[id]);
+        max_err = std::max(max_err, e);
+        sum_abs += e;
+        sum_ref += std::fabs((double)E.vss64[id]);
+        m++;
+      }
+      rel_err = m ? sum_abs / std::max(sum_ref, 1.0) : 0.0;
+      if (rel_err > gate) { fallback = 1; break; }
+      std::vector<int> more;
+      for (int c : rank)
+        if (!refined[c] && (double)cmin[c] - max_err <= (double)best) more.push_back(c);
+      if (more.empty()) break;
+      if (cells_refined + (int)more.size() > top_k + max_expand) { fallback = 1; break; }
+      TOMO_TRY(refine_cells(more));
+    }
+  }
+  if (fallback) {
+    std::vector<int> rest;
+    for (int id = 0; id < n; id++) if (!done[id]) rest.push_back(id);
+    TOMO_TRY(evaluate(rest));
+  }
+  E.finalize_host();
+  // _find1stOptimal over the evaluated orientations, in grid order
+  int opt = 0;
+  if (n > 1) {
+    float bestm = 1e5f;
+    for (int id = 0; id < n; id++)
+      if (done[id] && E.Mss[id] < bestm) { bestm = E.Mss[id]; opt = id; }
+  }
+  if (Mss_out)
+    for (int id = 0; id < n; id++) Mss_out[id] = done[id] ? E.Mss[id] : NAN;
+  if (pred_out) std::memcpy(pred_out, pred.data(), sizeof(float) * n);
+  if (stats) {
+    const double v[12] = {(double)evaluated.size(), (double)fallback, rel_err, max_err, (double)train_loss,
+                          seconds_since(t_start), t_exact, t_train, t_pred, (double)cells_refined, (double)rounds,
+                          (double)n_coarse};
+    std::memcpy(stats, v, sizeof(v));
+  }
+  return opt;
 }
 
 }  // extern "C"

@@ -1344,6 +1344,20 @@ cudaError_t launch_dump_gather(const int* cols8, const unsigned* keys64, const s
   return cudaGetLastError();
 }
 
+__global__ void k_zero_ids(int* out, const int* ids, int n)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[ids[i]] = 0;
+}
+
+// out[ids[i]] = 0 for i < n (per-orientation counters of a subset sweep).
+cudaError_t launch_zero_ids(int* out, const int* ids, int n, cudaStream_t s)
+{
+  if (n <= 0) return cudaSuccess;
+  k_zero_ids<<<(n + 255) / 256, 256, 0, s>>>(out, ids, n);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_fold(const EngineParams& p, cudaStream_t side, LaunchLog* L)
 {
   TOMO_LAUNCH(kKFold, side, (k_fold<<<p.Bo, 128, 0, side>>>(p)));

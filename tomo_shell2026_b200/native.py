@@ -63,6 +63,14 @@ EXPORTS = [
     ("tomoBatchConfig", ct.c_int, [ct.c_int, _i32p]),
     ("tomoBatchSetOption", ct.c_int, [ct.c_int, ct.c_int]),
     ("tomoBatchRelease", None, []),
+    ("tomoMlpInit", ct.c_int, [ct.c_int]),
+    ("tomoMlpParams", ct.c_int, [_f32p, _f32p]),
+    ("tomoMlpGrad", ct.c_int, [_f32p, _f32p, ct.c_int, _f32p, _f32p]),
+    ("tomoMlpAdam", ct.c_int, [ct.c_float]),
+    ("tomoMlpFit", ct.c_int, [_f32p, _f32p, ct.c_int, ct.c_int, ct.c_float, _f32p]),
+    ("tomoMlpPredict", ct.c_int, [_f32p, ct.c_int, _f32p]),
+    ("tomoSurrogateSearch", ct.c_int, [_f32p, _i32p, _f32p, _i32p, _f32p, _f32p, ct.c_int, ct.c_int, _i32p, _f32p,
+                                       _f32p, _f32p, ct.POINTER(ct.c_double)]),
 ]
 
 _LIB: ct.CDLL | None = None
