@@ -37,6 +37,11 @@ cudaError_t launch_bin_count(const EngineParams& p, cudaStream_t main, LaunchLog
 cudaError_t launch_after_count(const EngineParams& p, cudaStream_t main, size_t strip_smem, LaunchLog* L);
 cudaError_t launch_dump_scan(const int* cols8, int GG, int* off, int* totals, cudaStream_t s);
 cudaError_t launch_zero_ids(int* out, const int* ids, int n, cudaStream_t s);
+cudaError_t launch_gather_outputs(const long long* vo, const long long* vss, const long long* vtc, const long long* ent,
+                                  const long long* col, const float* vof, const float* vssf, const float* vtcf,
+                                  const int* nbed, const int* flags, const int* ids, int n, long long* stage,
+                                  cudaStream_t s);
+cudaError_t launch_scatter_rot(float* rot, const float* compact, const int* ids, int n, cudaStream_t s);
 cudaError_t launch_dump_gather(const int* cols8, const unsigned* keys64, const short* types64, int GG, const int* off,
                                int* cols9, unsigned* keys, short* types, cudaStream_t s);
 
@@ -292,6 +297,13 @@ struct Engine {
   DevBuf<long long> o_vo, o_vss, o_vtc, o_ent, o_col;
   DevBuf<float> o_vof, o_vssf, o_vtcf;
   DevBuf<int> o_nbed, o_flags;
+  // subset fetch (see fetch_subset) and lazy rotations (see ensure_rot)
+  DevBuf<int> sub_ids;
+  DevBuf<long long> sub_stage;
+  std::vector<int> sub_host;
+  int sub_n = 0;
+  std::vector<float> h_ypr;
+  std::vector<char> rot_ready;
 
   // host results of the last sweep
   Params P{};
@@ -319,6 +331,7 @@ struct Engine {
   void release()
   {
     vpos.release(); vnrm.release(); tri.release(); rot.release(); ori.release();
+    sub_ids.release(); sub_stage.release();
     o_vo.release(); o_vss.release(); o_vtc.release(); o_ent.release(); o_col.release();
     o_vof.release(); o_vssf.release(); o_vtcf.release(); o_nbed.release(); o_flags.release();
     if (owns_ws) W.release();
@@ -393,7 +406,7 @@ struct Engine {
   }
 
   int upload(const float* f32, const int* i32, const float* ypr, const int* tri_h, const float* vtx,
-             const float* vnrm_h)
+             const float* vnrm_h, bool lazy_rot = false)
   {
     P = read_params(f32, i32);
     if (P.n_tri < 0 || P.n_vtx < 0 || P.n_ypr < 0) return set_error(TOMO_ERR_ARG, "negative size in Int32Info");
@@ -433,7 +446,10 @@ struct Engine {
     std::vector<int4> ht(std::max(P.n_tri, 1));
     for (int t = 0; t < P.n_tri; t++) ht[t] = make_int4(tri_h[t * 3 + 0], tri_h[t * 3 + 1], tri_h[t * 3 + 2], 0);
     h_rot.assign((size_t)std::max(nYPR, 1) * 9, 0.f);
-    for (int i = 0; i < nYPR; i++) rotation(ypr[i * 3 + 0], ypr[i * 3 + 1], ypr[i * 3 + 2], &h_rot[(size_t)i * 9]);
+    rot_ready.assign((size_t)std::max(nYPR, 1), lazy_rot ? 0 : 1);
+    if (lazy_rot) h_ypr.assign(ypr, ypr + (size_t)nYPR * 3);
+    else
+      for (int i = 0; i < nYPR; i++) rotation(ypr[i * 3 + 0], ypr[i * 3 + 1], ypr[i * 3 + 2], &h_rot[(size_t)i * 9]);
     std::vector<int> hori(std::max(nYPR, 1));
     for (int i = 0; i < nYPR; i++) hori[i] = i;
 
@@ -442,7 +458,8 @@ struct Engine {
     TOMO_CUDA(cudaMemcpyAsync(vpos.ptr, hp.data(), sizeof(float4) * hp.size(), cudaMemcpyHostToDevice, main));
     TOMO_CUDA(cudaMemcpyAsync(vnrm.ptr, hn.data(), sizeof(float4) * hn.size(), cudaMemcpyHostToDevice, main));
     TOMO_CUDA(cudaMemcpyAsync(tri.ptr, ht.data(), sizeof(int4) * ht.size(), cudaMemcpyHostToDevice, main));
-    TOMO_CUDA(cudaMemcpyAsync(rot.ptr, h_rot.data(), sizeof(float) * h_rot.size(), cudaMemcpyHostToDevice, main));
+    if (!lazy_rot)
+      TOMO_CUDA(cudaMemcpyAsync(rot.ptr, h_rot.data(), sizeof(float) * h_rot.size(), cudaMemcpyHostToDevice, main));
     TOMO_CUDA(cudaMemcpyAsync(ori.ptr, hori.data(), sizeof(int) * hori.size(), cudaMemcpyHostToDevice, main));
     TOMO_CUDA(cudaStreamSynchronize(main));
     return 0;
@@ -595,8 +612,11 @@ struct Engine {
     return 0;
   }
 
+  // Per-orientation outputs to the host: all of them, or (after resolve has
+  // uploaded a subset to sub_ids) only the subset's, gathered on the device.
   int fetch()
   {
+    if (sub_n > 0) return fetch_subset();
     const size_t n = (size_t)nYPR;
     vo64.assign(n, 0); vss64.assign(n, 0); vtc64.assign(n, 0); entries.assign(n, 0); columns.assign(n, 0);
     vof.assign(n, 0.f); vssf.assign(n, 0.f); vtcf.assign(n, 0.f); nbed.assign(n, 0); flags.assign(n, 0);
@@ -617,6 +637,59 @@ struct Engine {
     return 0;
   }
 
+  int fetch_subset()
+  {
+    const size_t n = (size_t)nYPR, k = (size_t)sub_n;
+    if (vo64.size() != n) {
+      vo64.assign(n, 0); vss64.assign(n, 0); vtc64.assign(n, 0); entries.assign(n, 0); columns.assign(n, 0);
+      vof.assign(n, 0.f); vssf.assign(n, 0.f); vtcf.assign(n, 0.f); nbed.assign(n, 0); flags.assign(n, 0);
+    }
+    if (P.n_tri == 0) return 0;
+    TOMO_CUDA(sub_stage.reserve(k * 10));
+    TOMO_CUDA(launch_gather_outputs(o_vo.ptr, o_vss.ptr, o_vtc.ptr, o_ent.ptr, o_col.ptr, o_vof.ptr, o_vssf.ptr,
+                                    o_vtcf.ptr, o_nbed.ptr, o_flags.ptr, sub_ids.ptr, sub_n, sub_stage.ptr, main));
+    std::vector<long long> h(k * 10);
+    TOMO_CUDA(cudaMemcpyAsync(h.data(), sub_stage.ptr, sizeof(long long) * h.size(), cudaMemcpyDeviceToHost, main));
+    TOMO_CUDA(cudaStreamSynchronize(main));
+    TOMO_CUDA(cudaStreamSynchronize(side));
+    auto f = [](long long b) { const int i = (int)b; float x; std::memcpy(&x, &i, sizeof(x)); return x; };
+    for (size_t q = 0; q < k; q++) {
+      const int id = sub_host[q];
+      const long long* r = &h[q * 10];
+      vo64[id] = r[0]; vss64[id] = r[1]; vtc64[id] = r[2]; entries[id] = r[3]; columns[id] = r[4];
+      vof[id] = f(r[5]); vssf[id] = f(r[6]); vtcf[id] = f(r[7]); nbed[id] = (int)r[8]; flags[id] = (int)r[9];
+    }
+    log.collect();
+    return 0;
+  }
+
+  // Rotation matrices computed on the host and uploaded only for the listed
+  // orientations (uploads made with lazy rotations).
+  int ensure_rot(const std::vector<int>& ids)
+  {
+    std::vector<int> need;
+    std::vector<float> compact;
+    for (int id : ids) {
+      if (rot_ready[id]) continue;
+      rotation(h_ypr[id * 3 + 0], h_ypr[id * 3 + 1], h_ypr[id * 3 + 2], &h_rot[(size_t)id * 9]);
+      rot_ready[id] = 1;
+      need.push_back(id);
+      compact.insert(compact.end(), &h_rot[(size_t)id * 9], &h_rot[(size_t)id * 9] + 9);
+    }
+    if (need.empty()) return 0;
+    DevBuf<int> di;
+    DevBuf<float> dc;
+    TOMO_CUDA(di.reserve(need.size()));
+    TOMO_CUDA(dc.reserve(compact.size()));
+    TOMO_CUDA(cudaMemcpyAsync(di.ptr, need.data(), sizeof(int) * need.size(), cudaMemcpyHostToDevice, main));
+    TOMO_CUDA(cudaMemcpyAsync(dc.ptr, compact.data(), sizeof(float) * compact.size(), cudaMemcpyHostToDevice, main));
+    TOMO_CUDA(launch_scatter_rot(rot.ptr, dc.ptr, di.ptr, (int)need.size(), main));
+    TOMO_CUDA(cudaStreamSynchronize(main));
+    di.release();
+    dc.release();
+    return 0;
+  }
+
   // Full device phase: the sweep in configuration 0, then the re-runs of
   // flagged orientations: overflowed strip lists in configuration 2, stray
   // hits and priority-dependent columns in configuration 1, and what still
@@ -633,11 +706,25 @@ struct Engine {
   {
     for (int& r : n_redo) r = 0;
     std::vector<int> all;
+    sub_n = 0;
     if (!subset) {
       all.resize(nYPR);
       for (int i = 0; i < nYPR; i++) all[i] = i;
       subset = &all;
+    } else if (!subset->empty()) {
+      TOMO_CUDA(sub_ids.reserve(subset->size()));
+      TOMO_CUDA(cudaMemcpyAsync(sub_ids.ptr, subset->data(), sizeof(int) * subset->size(), cudaMemcpyHostToDevice, main));
+      sub_host = *subset;
+      sub_n = (int)subset->size();
     }
+    const int rc = resolve_ids(*subset);
+    sub_n = 0;
+    return rc;
+  }
+
+  int resolve_ids(const std::vector<int>& ids)
+  {
+    const std::vector<int>* subset = &ids;
     std::vector<int> big, safe, narrow;
     if (force_safe) {
       if (nYPR == 0 || P.n_tri == 0) return fetch();
@@ -1864,6 +1951,7 @@ double seconds_since(std::chrono::steady_clock::time_point t0)
 int eval_ids(Engine& E, const std::vector<int>& ids, DevBuf<int>& dids)
 {
   if (ids.empty()) return 0;
+  TOMO_TRY(E.ensure_rot(ids));
   TOMO_CUDA(dids.reserve(ids.size()));
   TOMO_CUDA(cudaMemcpyAsync(dids.ptr, ids.data(), sizeof(int) * ids.size(), cudaMemcpyHostToDevice, E.main));
   TOMO_TRY(E.sweep_device(dids.ptr, (int)ids.size()));
@@ -1962,7 +2050,7 @@ int tomoSurrogateSearch(const float* f32info, const int* i32info, const float* Y
   if (cell < 1 || top_k < 1 || steps < 0 || max_expand < 0) return set_error(TOMO_ERR_ARG, "bad search parameters");
   Engine& E = engine();
   TOMO_TRY(E.init());
-  TOMO_TRY(E.upload(f32info, i32info, YPR, tri, vtx, vtx_nrm));
+  TOMO_TRY(E.upload(f32info, i32info, YPR, tri, vtx, vtx_nrm, true));
   const int n = E.nYPR;
   double t_exact = 0.0, t_train = 0.0, t_pred = 0.0;
   std::vector<char> done(n, 0);
@@ -1992,11 +2080,17 @@ int tomoSurrogateSearch(const float* f32info, const int* i32info, const float* Y
       for (int iy = 0; iy < n_yaw; iy += cell) coarse.push_back(ip * n_yaw + iy);
     n_coarse = (int)coarse.size();
     TOMO_TRY(evaluate(coarse));
-    // 2. train on standardised exact Vss
-    auto feat = [&](int id, float* f) {
-      const float y = YPR[id * 3 + 0], p = YPR[id * 3 + 1];
-      f[0] = sinf(y); f[1] = cosf(y); f[2] = sinf(p); f[3] = cosf(p);
-    };
+    // 2. features of every grid point on the device (the same bits for
+    //    training and prediction); train on standardised exact Vss
+    DevBuf<float> dypr, dx, dy;
+    TOMO_CUDA(dypr.reserve((size_t)n * 3));
+    TOMO_CUDA(dx.reserve((size_t)n * kMlpIn));
+    TOMO_CUDA(dy.reserve((size_t)n));
+    TOMO_CUDA(cudaMemcpyAsync(dypr.ptr, YPR, sizeof(float) * n * 3, cudaMemcpyHostToDevice, E.main));
+    TOMO_CUDA(mlp_features(dypr.ptr, n, dx.ptr, E.main));
+    std::vector<float> F((size_t)n * kMlpIn);
+    TOMO_CUDA(cudaMemcpyAsync(F.data(), dx.ptr, sizeof(float) * F.size(), cudaMemcpyDeviceToHost, E.main));
+    TOMO_CUDA(cudaStreamSynchronize(E.main));
     double mean = 0.0, sq = 0.0;
     for (int id : coarse) mean += (double)E.vss64[id];
     mean /= (double)coarse.size();
@@ -2004,7 +2098,7 @@ int tomoSurrogateSearch(const float* f32info, const int* i32info, const float* Y
     const double sd = coarse.size() > 1 && sq > 0.0 ? std::sqrt(sq / (double)coarse.size()) : 1.0;
     std::vector<float> X(coarse.size() * kMlpIn), Y(coarse.size());
     for (size_t k = 0; k < coarse.size(); k++) {
-      feat(coarse[k], &X[k * kMlpIn]);
+      std::memcpy(&X[k * kMlpIn], &F[(size_t)coarse[k] * kMlpIn], sizeof(float) * kMlpIn);
       Y[k] = (float)(((double)E.vss64[coarse[k]] - mean) / sd);
     }
     {
@@ -2017,20 +2111,15 @@ int tomoSurrogateSearch(const float* f32info, const int* i32info, const float* Y
     // 3. predict every grid point
     {
       const auto t0 = std::chrono::steady_clock::now();
-      std::vector<float> F((size_t)n * kMlpIn);
-      for (int id = 0; id < n; id++) feat(id, &F[(size_t)id * kMlpIn]);
-      DevBuf<float> dx, dy;
-      TOMO_CUDA(dx.reserve(F.size()));
-      TOMO_CUDA(dy.reserve((size_t)n));
-      TOMO_CUDA(cudaMemcpyAsync(dx.ptr, F.data(), sizeof(float) * F.size(), cudaMemcpyHostToDevice, E.main));
       TOMO_CUDA(mlp().predict_device(dx.ptr, n, dy.ptr, E.main));
       TOMO_CUDA(cudaMemcpyAsync(pred.data(), dy.ptr, sizeof(float) * n, cudaMemcpyDeviceToHost, E.main));
       TOMO_CUDA(cudaStreamSynchronize(E.main));
-      dx.release();
-      dy.release();
       for (int id = 0; id < n; id++) pred[id] = (float)(pred[id] * sd + mean);
       t_pred += seconds_since(t0);
     }
+    dypr.release();
+    dx.release();
+    dy.release();
     // 4. cells by smallest prediction; refine the top_k
     std::vector<float> cmin(ncell, INFINITY);
     for (int id = 0; id < n; id++) { const int c = cell_of(id); cmin[c] = std::min(cmin[c], pred[id]); }

@@ -1344,6 +1344,45 @@ cudaError_t launch_dump_gather(const int* cols8, const unsigned* keys64, const s
   return cudaGetLastError();
 }
 
+// stage[k][10] = the per-orientation outputs of orientation ids[k] (floats as bits).
+__global__ void k_gather_outputs(const long long* vo, const long long* vss, const long long* vtc, const long long* ent,
+                                 const long long* col, const float* vof, const float* vssf, const float* vtcf,
+                                 const int* nbed, const int* flags, const int* ids, int n, long long* stage)
+{
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const int id = ids[k];
+  long long* o = stage + (size_t)k * 10;
+  o[0] = vo[id]; o[1] = vss[id]; o[2] = vtc[id]; o[3] = ent[id]; o[4] = col[id];
+  o[5] = __float_as_int(vof[id]); o[6] = __float_as_int(vssf[id]); o[7] = __float_as_int(vtcf[id]);
+  o[8] = nbed[id]; o[9] = flags[id];
+}
+
+cudaError_t launch_gather_outputs(const long long* vo, const long long* vss, const long long* vtc, const long long* ent,
+                                  const long long* col, const float* vof, const float* vssf, const float* vtcf,
+                                  const int* nbed, const int* flags, const int* ids, int n, long long* stage,
+                                  cudaStream_t s)
+{
+  if (n <= 0) return cudaSuccess;
+  k_gather_outputs<<<(n + 255) / 256, 256, 0, s>>>(vo, vss, vtc, ent, col, vof, vssf, vtcf, nbed, flags, ids, n, stage);
+  return cudaGetLastError();
+}
+
+// rot[ids[k]] = compact[k] (9 floats each): rotation matrices uploaded on demand.
+__global__ void k_scatter_rot(float* rot, const float* compact, const int* ids, int n)
+{
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n * 9) return;
+  rot[(size_t)ids[e / 9] * 9 + e % 9] = compact[e];
+}
+
+cudaError_t launch_scatter_rot(float* rot, const float* compact, const int* ids, int n, cudaStream_t s)
+{
+  if (n <= 0) return cudaSuccess;
+  k_scatter_rot<<<(n * 9 + 255) / 256, 256, 0, s>>>(rot, compact, ids, n);
+  return cudaGetLastError();
+}
+
 __global__ void k_zero_ids(int* out, const int* ids, int n)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;

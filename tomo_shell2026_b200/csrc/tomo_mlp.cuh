@@ -1,10 +1,12 @@
 // Surrogate network of the learned-proposal orientation search: an FP32 MLP
 // [sin yaw, cos yaw, sin pitch, cos pitch] -> 128 -> 128 -> 128 -> Vss with
 // tanh hidden units and a linear output, trained full-batch with Adam by the
-// hand-written kernels of tomo_mlp.cu (tiled SIMT GEMMs with fused bias /
-// activation / activation-derivative epilogues, column sums, MSE gradient,
-// Adam).  Nothing here is a dense contraction large enough for tensor cores:
-// one training step is ~60 MFLOP.
+// hand-written kernels of tomo_mlp.cu: one fused kernel per block of 16
+// samples runs the forward pass, the loss and the whole backward pass out of
+// shared memory and writes that block's gradient; a second kernel sums the
+// blocks' gradients in a fixed order (deterministic) and applies Adam.
+// Nothing here is a dense contraction large enough for tensor cores: one
+// training step on 936 samples is ~60 MFLOP.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -25,6 +27,9 @@ struct MlpLayout {
   MlpLayout();
 };
 
+// x[n][4] = sin yaw, cos yaw, sin pitch, cos pitch of ypr[n][3] (device arrays).
+cudaError_t mlp_features(const float* ypr, int n, float* x, cudaStream_t s);
+
 class Mlp {
  public:
   ~Mlp();
@@ -43,7 +48,7 @@ class Mlp {
   cudaError_t read_grad(float* host, float* loss, cudaStream_t s);
   // One Adam step from the current gradient.
   cudaError_t adam(float lr, cudaStream_t s);
-  // steps x (grad + Adam), replayed from one captured CUDA graph per step.
+  // steps x (grad + Adam).
   cudaError_t fit(int steps, float lr, cudaStream_t s, float* final_loss);
   // Prediction for n device feature rows.
   cudaError_t predict_device(const float* dev_x, int n, float* dev_out, cudaStream_t s);
@@ -52,19 +57,14 @@ class Mlp {
 
  private:
   cudaError_t reserve(int n);
-  cudaError_t forward(const float* x, int n, float* out, cudaStream_t s);
+  cudaError_t step(float lr, bool update, cudaStream_t s);
   void free_all();
 
-  float *params_ = nullptr, *grads_ = nullptr, *m_ = nullptr, *v_ = nullptr;
+  float *params_ = nullptr, *wt_ = nullptr;   // parameters, and each weight matrix transposed ([out][in])
+  float *grads_ = nullptr, *m_ = nullptr, *v_ = nullptr;
   float *x_ = nullptr, *y_ = nullptr, *loss_ = nullptr;
-  float *act_[kMlpLayers] = {nullptr, nullptr, nullptr, nullptr};   // tanh outputs of layers 1..3, output of layer 4
-  float *dz_[2] = {nullptr, nullptr};
-  int* step_ = nullptr;
-  int cap_ = 0, n_ = 0;
-  cudaGraphExec_t step_exec_ = nullptr;
-  cudaGraph_t step_graph_ = nullptr;
-  float step_lr_ = -1.f;
-  int step_n_ = -1;
+  float *part_ = nullptr, *part_loss_ = nullptr;   // per-block gradients [blocks][total], losses [blocks]
+  int cap_ = 0, n_ = 0, steps_done_ = 0;
 };
 
 }  // namespace tomo
