@@ -318,8 +318,48 @@ def run_ours(args, rank, world, local_rank):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(mesh, ypr, opts, grid, budget_s=args.cpu_budget_s,
                                             gpu_vss=res["Vss64"])
+    if world == 1 and not args.no_extras:
+        line["plain"] = plain_rate(mesh, ypr, opts)
+        from tomo_shell2026_b200 import suites
+        line["batched"] = suites.batched_suite(n_meshes=args.batched_meshes)
+        line["surrogate"] = suites.surrogate_suite(n_meshes=args.surrogate_meshes)
     if rank == 0:
         print(json.dumps(line), flush=True)
+    return 0
+
+
+def plain_rate(mesh, ypr, opts, n: int = 256) -> dict:
+    """The same sweep launched one orientation at a time (every kernel of the
+    pipeline per orientation, as a per-orientation engine does), on an evenly
+    strided sample of the grid: device orientations/s."""
+    from tomo_shell2026_b200 import native
+    sub = np.ascontiguousarray(ypr[np.linspace(0, ypr.shape[0] - 1, n).astype(np.int64)])
+    native.set_option(native.TOMO_OPT_BATCH, 1)
+    try:
+        s = native.Session(mesh, sub, opts)
+        s.run_device()
+        ms = s.run_device()
+    finally:
+        native.set_option(native.TOMO_OPT_BATCH, 128)
+    return {"orientations": n, "orientations_per_s": n / (ms / 1000.0), "orientations_per_launch": 1}
+
+
+def run_suite(args) -> int:
+    """Full-size suites, one JSON line each (not part of the default run)."""
+    import torch
+    from tomo_shell2026_b200 import suites
+    torch.cuda.set_device(0)
+    if args.suite == "batched":
+        r = suites.batched_suite(n_meshes=64)
+        line = {"metric": "aggregate orientations/s, 64 uneven meshes (1k-120k tris), 1deg grid, one graph launch",
+                "value": r["batched_orientations_per_s"], "unit": "orientations/s", "higher_is_better": True,
+                "suite": r}
+    else:
+        r = suites.surrogate_suite(n_meshes=100)
+        line = {"metric": "learned-proposal search: meshes reaching the exhaustive optimum in <= 1/5 of its time",
+                "value": r["meshes_at_target"], "unit": "fraction of 100 meshes", "higher_is_better": True,
+                "suite": r}
+    print(json.dumps(line), flush=True)
     return 0
 
 
@@ -364,6 +404,12 @@ def main():
     ap.add_argument("--cpu-budget-s", type=float, default=15.0)
     ap.add_argument("--ref-step-s", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the plain-launch, batched and surrogate figures added to the line")
+    ap.add_argument("--batched-meshes", type=int, default=16)
+    ap.add_argument("--surrogate-meshes", type=int, default=10)
+    ap.add_argument("--suite", choices=("none", "batched", "surrogate"), default="none",
+                    help="run a full-size suite instead (64 uneven meshes / 100 searched meshes)")
     ap.add_argument("--max-orientations", type=int, default=0,
                     help="keep only the first N orientations (small profiling cases; 0 = the whole grid)")
     args = ap.parse_args()
@@ -372,6 +418,8 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference(args, rank)
+    if args.suite != "none":
+        return run_suite(args) if rank == 0 else 0
     if world > 1:
         import datetime
 

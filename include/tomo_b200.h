@@ -181,20 +181,27 @@ int tomoMlpFit(const float* x, const float* y, int n, int steps, float lr, float
 int tomoMlpPredict(const float* x, int n, float* out);
 
 /* Learned-proposal search over a YPR grid laid out [n_pitch][n_yaw] (yaw
- * fastest; n_yaw * n_pitch = Int32Info[6]): the exact kernels evaluate the
- * coarse points (both indices multiples of `cell`), the network is trained on
- * their exact Vss, ranks the cell x cell blocks by predicted Vss, the top_k
- * blocks are evaluated exactly, then every block whose smallest prediction is
- * within the largest observed out-of-sample error of the best exact Vss, round
- * after round; more than max_expand extra blocks, a mean relative error above
- * `gate`, or a bed (Mss then not monotone in Vss) fall back to the exhaustive
- * sweep.  iparams = {cell, top_k, train_steps, seed, max_expand},
- * fparams = {learning_rate, gate}.  Returns optID (_find1stOptimal over the
- * evaluated orientations, grid order).  Mss_out[nYPR]: exact Mss where
- * evaluated, NaN elsewhere; pred_out[nYPR]: predicted Vss (either may be
- * null).  stats[12] = evaluated orientations, fell back (0/1), mean relative
- * error, max abs error, final training loss, seconds total / exact sweeps /
- * training / prediction, blocks refined, expansion rounds, coarse points. */
+ * fastest; n_yaw * n_pitch = Int32Info[6]).  The exact kernels evaluate the
+ * coarse points (both grid indices multiples of `stride`); the network is
+ * trained on their exact Vss, except a seeded `holdout` share kept to measure
+ * its error; it ranks the cell x cell blocks of the grid by their smallest
+ * predicted Vss and the top_k blocks are evaluated exactly.  Then, round
+ * after round, every block whose smallest prediction minus margin x (largest
+ * error seen on any evaluated point not trained on) is at or below the best
+ * exact Vss is evaluated too.  The search falls back to the exhaustive sweep
+ * when that would exceed max_eval evaluated orientations (0 = nYPR / 5), when
+ * the mean relative error of the untrained points exceeds `gate`, or with a
+ * bed (Mss is then not a function of Vss alone).
+ * iparams = {stride, cell, top_k, train_steps, seed, max_eval},
+ * fparams = {learning_rate, gate, margin, holdout, log_scale}: with
+ * log_scale > 0 the network learns log1p((Vss - min) / s), s = log_scale x
+ * (median - min) of its training Vss, instead of Vss.  Returns optID
+ * (_find1stOptimal over the evaluated orientations, grid order).
+ * Mss_out[nYPR]: exact Mss where evaluated, NaN elsewhere; pred_out[nYPR]:
+ * predicted Vss (either may be null).  stats[12] = evaluated orientations,
+ * fell back (0/1), mean relative error, max abs error, final training loss,
+ * seconds total / exact sweeps / training / prediction, blocks refined,
+ * expansion rounds, coarse points. */
 int tomoSurrogateSearch(const float* f32info, const int* i32info, const float* YPR, const int* tri, const float* vtx,
                         const float* vtx_nrm, int n_yaw, int n_pitch, const int* iparams, const float* fparams,
                         float* Mss_out, float* pred_out, double* stats);

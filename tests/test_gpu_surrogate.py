@@ -77,7 +77,7 @@ def test_search_reaches_the_exhaustive_optimum(seed):
     ypr = meshgen.ypr_grid(np.arange(0, 360), np.arange(0, 61))
     opts = PrintOptions(explicit_ss=True)
     ex = native.sweep(mesh, ypr, opts)
-    r = surrogate.search(mesh, ypr, n_yaw, n_pitch, opts, cell=5, top_k=8, steps=300, seed=seed)
+    r = surrogate.search(mesh, ypr, n_yaw, n_pitch, opts, stride=5, cell=5, top_k=16, seed=seed)
     assert np.float32(r.Mss[r.optID]) == ex.Mss[ex.optID], "optimum value differs from the exhaustive sweep"
     done = ~np.isnan(r.Mss)
     assert np.array_equal(r.Mss[done].view(np.int32), ex.Mss[done].view(np.int32)), "evaluated Mss not exact"
@@ -92,6 +92,6 @@ def test_bed_falls_back_to_exhaustive():
     ypr = meshgen.ypr_grid(np.arange(0, 360, 10), np.arange(0, 70, 10))
     opts = PrintOptions(bed_type=2, bed_outer=2.0, bed_thickness=0.97)
     ex = native.sweep(mesh, ypr, opts)
-    r = surrogate.search(mesh, ypr, 36, 7, opts, cell=2)
+    r = surrogate.search(mesh, ypr, 36, 7, opts, stride=2, cell=2)
     assert r.fallback and r.evaluated == ypr.shape[0]
     assert r.optID == ex.optID and np.array_equal(r.Mss.view(np.int32), ex.Mss.view(np.int32))

@@ -2043,17 +2043,20 @@ int tomoSurrogateSearch(const float* f32info, const int* i32info, const float* Y
   const auto t_start = std::chrono::steady_clock::now();
   if (f32info == nullptr || i32info == nullptr || iparams == nullptr || fparams == nullptr)
     return set_error(TOMO_ERR_ARG, "null argument");
-  const int cell = iparams[0], top_k = iparams[1], steps = iparams[2], seed = iparams[3], max_expand = iparams[4];
-  const float lr = fparams[0], gate = fparams[1];
+  const int stride = iparams[0], cell = iparams[1], top_k = iparams[2], steps = iparams[3], seed = iparams[4];
+  const float lr = fparams[0], gate = fparams[1], margin = fparams[2], holdout = fparams[3], log_scale = fparams[4];
   if (n_yaw <= 0 || n_pitch <= 0 || (long long)n_yaw * n_pitch != i32info[6])
     return set_error(TOMO_ERR_ARG, "n_yaw * n_pitch must equal nYPR");
-  if (cell < 1 || top_k < 1 || steps < 0 || max_expand < 0) return set_error(TOMO_ERR_ARG, "bad search parameters");
+  if (stride < 1 || cell < 1 || top_k < 1 || steps < 0 || iparams[5] < 0 || !(margin >= 0.f) || !(holdout >= 0.f) ||
+      holdout >= 0.9f)
+    return set_error(TOMO_ERR_ARG, "bad search parameters");
   Engine& E = engine();
   TOMO_TRY(E.init());
   TOMO_TRY(E.upload(f32info, i32info, YPR, tri, vtx, vtx_nrm, true));
   const int n = E.nYPR;
+  const int budget = iparams[5] > 0 ? iparams[5] : std::max(1, n / 5);
   double t_exact = 0.0, t_train = 0.0, t_pred = 0.0;
-  std::vector<char> done(n, 0);
+  std::vector<char> done(n, 0), trained(n, 0);
   std::vector<int> evaluated;
   DevBuf<int> dids;
   auto evaluate = [&](const std::vector<int>& ids) -> int {
@@ -2074,14 +2077,16 @@ int tomoSurrogateSearch(const float* f32info, const int* i32info, const float* Y
   if (E.P.bed_type != kBedNone || E.P.n_tri == 0) {
     fallback = 1;
   } else {
-    // 1. coarse points, exact
+    // 1. coarse points (both grid indices multiples of `stride`), exact
     std::vector<int> coarse;
-    for (int ip = 0; ip < n_pitch; ip += cell)
-      for (int iy = 0; iy < n_yaw; iy += cell) coarse.push_back(ip * n_yaw + iy);
+    for (int ip = 0; ip < n_pitch; ip += stride)
+      for (int iy = 0; iy < n_yaw; iy += stride) coarse.push_back(ip * n_yaw + iy);
     n_coarse = (int)coarse.size();
     TOMO_TRY(evaluate(coarse));
     // 2. features of every grid point on the device (the same bits for
-    //    training and prediction); train on standardised exact Vss
+    //    training and prediction); a seeded share of the coarse points is
+    //    held out of training so the prediction error is also measured away
+    //    from the refined cells; train on standardised exact Vss
     DevBuf<float> dypr, dx, dy;
     TOMO_CUDA(dypr.reserve((size_t)n * 3));
     TOMO_CUDA(dx.reserve((size_t)n * kMlpIn));
@@ -2091,20 +2096,41 @@ int tomoSurrogateSearch(const float* f32info, const int* i32info, const float* Y
     std::vector<float> F((size_t)n * kMlpIn);
     TOMO_CUDA(cudaMemcpyAsync(F.data(), dx.ptr, sizeof(float) * F.size(), cudaMemcpyDeviceToHost, E.main));
     TOMO_CUDA(cudaStreamSynchronize(E.main));
+    std::vector<int> train;
+    {
+      unsigned h = 2166136261u ^ (unsigned)seed;
+      for (int id : coarse) {
+        h = (h ^ (unsigned)id) * 16777619u;   // FNV-1a step: a fixed pseudo-random split
+        const float u = (float)((h >> 8) & 0xFFFF) / 65536.f;
+        if (u >= holdout) { train.push_back(id); trained[id] = 1; }
+      }
+      if (train.empty()) { train = coarse; for (int id : coarse) trained[id] = 1; }
+    }
+    // target: Vss, or with log_scale > 0 log1p((Vss - min) / s), s = log_scale x
+    // (median - min) of the training Vss, which spends the network's accuracy
+    // near the minimum; then standardised
+    std::vector<double> tv;
+    for (int id : train) tv.push_back((double)E.vss64[id]);
+    std::vector<double> sorted_tv = tv;
+    std::sort(sorted_tv.begin(), sorted_tv.end());
+    const double vmin = sorted_tv.front();
+    const double tscale = log_scale > 0.f ? std::max(1.0, (double)log_scale * (sorted_tv[sorted_tv.size() / 2] - vmin)) : 0.0;
+    auto fwd = [&](double v) { return tscale > 0.0 ? std::log1p((v - vmin) / tscale) : v; };
+    auto inv = [&](double y) { return tscale > 0.0 ? vmin + tscale * std::expm1(y) : y; };
     double mean = 0.0, sq = 0.0;
-    for (int id : coarse) mean += (double)E.vss64[id];
-    mean /= (double)coarse.size();
-    for (int id : coarse) sq += ((double)E.vss64[id] - mean) * ((double)E.vss64[id] - mean);
-    const double sd = coarse.size() > 1 && sq > 0.0 ? std::sqrt(sq / (double)coarse.size()) : 1.0;
-    std::vector<float> X(coarse.size() * kMlpIn), Y(coarse.size());
-    for (size_t k = 0; k < coarse.size(); k++) {
-      std::memcpy(&X[k * kMlpIn], &F[(size_t)coarse[k] * kMlpIn], sizeof(float) * kMlpIn);
-      Y[k] = (float)(((double)E.vss64[coarse[k]] - mean) / sd);
+    for (double v : tv) mean += fwd(v);
+    mean /= (double)tv.size();
+    for (double v : tv) sq += (fwd(v) - mean) * (fwd(v) - mean);
+    const double sd = tv.size() > 1 && sq > 0.0 ? std::sqrt(sq / (double)tv.size()) : 1.0;
+    std::vector<float> X(train.size() * kMlpIn), Y(train.size());
+    for (size_t k = 0; k < train.size(); k++) {
+      std::memcpy(&X[k * kMlpIn], &F[(size_t)train[k] * kMlpIn], sizeof(float) * kMlpIn);
+      Y[k] = (float)((fwd(tv[k]) - mean) / sd);
     }
     {
       const auto t0 = std::chrono::steady_clock::now();
       TOMO_CUDA(mlp().init((unsigned)seed, E.main));
-      TOMO_CUDA(mlp().set_data(X.data(), Y.data(), (int)coarse.size(), E.main));
+      TOMO_CUDA(mlp().set_data(X.data(), Y.data(), (int)train.size(), E.main));
       TOMO_CUDA(mlp().fit(steps, lr, E.main, &train_loss));
       t_train += seconds_since(t0);
     }
@@ -2114,7 +2140,7 @@ int tomoSurrogateSearch(const float* f32info, const int* i32info, const float* Y
       TOMO_CUDA(mlp().predict_device(dx.ptr, n, dy.ptr, E.main));
       TOMO_CUDA(cudaMemcpyAsync(pred.data(), dy.ptr, sizeof(float) * n, cudaMemcpyDeviceToHost, E.main));
       TOMO_CUDA(cudaStreamSynchronize(E.main));
-      for (int id = 0; id < n; id++) pred[id] = (float)(pred[id] * sd + mean);
+      for (int id = 0; id < n; id++) pred[id] = (float)inv(pred[id] * sd + mean);
       t_pred += seconds_since(t0);
     }
     dypr.release();
@@ -2127,6 +2153,8 @@ int tomoSurrogateSearch(const float* f32info, const int* i32info, const float* Y
     for (int c = 0; c < ncell; c++) rank[c] = c;
     std::stable_sort(rank.begin(), rank.end(), [&](int a, int b) { return cmin[a] < cmin[b]; });
     std::vector<char> refined(ncell, 0);
+    std::vector<int> cell_todo(ncell, 0);
+    for (int id = 0; id < n; id++) if (!done[id]) cell_todo[cell_of(id)]++;
     auto refine_cells = [&](const std::vector<int>& cells) -> int {
       std::vector<int> ids;
       for (int c : cells) refined[c] = 1;
@@ -2137,7 +2165,8 @@ int tomoSurrogateSearch(const float* f32info, const int* i32info, const float* Y
     };
     std::vector<int> first(rank.begin(), rank.begin() + std::min(top_k, ncell));
     TOMO_TRY(refine_cells(first));
-    // 5. error gate and expansion
+    // 5. error gate and expansion: every untrained evaluated point (held-out
+    //    coarse points and refined points) measures the prediction error
     for (;; rounds++) {
       double sum_abs = 0.0, sum_ref = 0.0;
       max_err = 0.0;
@@ -2145,7 +2174,7 @@ int tomoSurrogateSearch(const float* f32info, const int* i32info, const float* Y
       int m = 0;
       for (int id : evaluated) {
         best = std::min(best, E.vss64[id]);
-        if ((id % n_yaw) % cell == 0 && (id / n_yaw) % cell == 0) continue;   // training point
+        if (trained[id]) continue;
         const double e = std::fabs((double)pred[id] - (double)E.vss64[id]);
         max_err = std::max(max_err, e);
         sum_abs += e;
@@ -2155,17 +2184,24 @@ int tomoSurrogateSearch(const float* f32info, const int* i32info, const float* Y
       rel_err = m ? sum_abs / std::max(sum_ref, 1.0) : 0.0;
       if (rel_err > gate) { fallback = 1; break; }
       std::vector<int> more;
+      long long extra = 0;
       for (int c : rank)
-        if (!refined[c] && (double)cmin[c] - max_err <= (double)best) more.push_back(c);
+        if (!refined[c] && (double)cmin[c] - margin * max_err <= (double)best) { more.push_back(c); extra += cell_todo[c]; }
       if (more.empty()) break;
-      if (cells_refined + (int)more.size() > top_k + max_expand) { fallback = 1; break; }
+      if ((long long)evaluated.size() + extra > budget) { fallback = 1; break; }
       TOMO_TRY(refine_cells(more));
     }
   }
   if (fallback) {
-    std::vector<int> rest;
-    for (int id = 0; id < n; id++) if (!done[id]) rest.push_back(id);
-    TOMO_TRY(evaluate(rest));
+    // the exhaustive sweep itself, over the whole grid
+    const auto t0 = std::chrono::steady_clock::now();
+    std::vector<int> all(n);
+    for (int id = 0; id < n; id++) all[id] = id;
+    TOMO_TRY(E.ensure_rot(all));
+    TOMO_TRY(E.sweep_device());
+    TOMO_TRY(E.resolve());
+    t_exact += seconds_since(t0);
+    for (int id = 0; id < n; id++) if (!done[id]) { done[id] = 1; evaluated.push_back(id); }
   }
   E.finalize_host();
   // _find1stOptimal over the evaluated orientations, in grid order

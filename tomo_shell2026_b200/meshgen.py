@@ -27,8 +27,9 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-__all__ = ["MeshArrays", "icosphere", "perturbed_icosphere", "ypr_grid", "small_solid",
-           "solid_82k", "random_mesh", "mesh_from_arrays"]
+__all__ = ["MeshArrays", "icosphere", "geodesic_sphere", "perturbed_icosphere", "uv_sphere", "perturbed_sphere",
+           "ypr_grid",
+           "small_solid", "solid_82k", "random_mesh", "mesh_from_arrays"]
 
 
 @dataclass
@@ -147,8 +148,87 @@ def perturbed_icosphere(subdivisions: int, radius: float, seed: int, n_harmonics
     """Closed icosphere, radially displaced by seeded real spherical harmonics
     (and optionally Gaussian bumps/dents), coordinates multiplied by ``scale``
     (2.0 expresses 0.5 mm voxels on the reference's 1-unit grid)."""
-    rng = np.random.default_rng(seed)
     u, f = icosphere(subdivisions)
+    return _perturbed(u, f, radius, seed, n_harmonics, max_degree, amplitude, n_bumps, bump_sigma, bump_height,
+                      scale, name or f"ico{subdivisions}_s{seed}", with_hull)
+
+
+def geodesic_sphere(frequency: int) -> tuple[np.ndarray, np.ndarray]:
+    """Unit geodesic sphere: every icosahedron face cut into frequency^2
+    triangles (20 * frequency^2 faces, outward winding, vertex valence 5 or 6),
+    points placed on each flat face and projected onto the sphere."""
+    nu = max(1, int(frequency))
+    base_v, base_f = icosphere(0)
+    ii, jj = np.meshgrid(np.arange(nu + 1), np.arange(nu + 1), indexing="ij")
+    keep = (ii + jj) <= nu
+    ii, jj = ii[keep], jj[keep]
+    local = -np.ones((nu + 1, nu + 1), np.int64)
+    local[ii, jj] = np.arange(ii.size)
+    pts = []
+    for a, b, c in base_f:
+        A, B, C = base_v[a], base_v[b], base_v[c]
+        P = A[None, :] + np.outer(ii / nu, B - A) + np.outer(jj / nu, C - A)
+        pts.append(P / np.linalg.norm(P, axis=1)[:, None])
+    pts = np.concatenate(pts)
+    _, first, inv = np.unique(np.round(pts, 9), axis=0, return_index=True, return_inverse=True)
+    inv = inv.reshape(-1)
+    order = np.argsort(first)
+    rank = np.empty_like(order)
+    rank[order] = np.arange(order.size)
+    gid = rank[inv]
+    verts = pts[first[order]]
+    tris = []
+    ti, tj = np.meshgrid(np.arange(nu), np.arange(nu), indexing="ij")
+    up = (ti + tj) <= nu - 1
+    dn = (ti + tj) <= nu - 2
+    for k in range(len(base_f)):
+        off = k * ii.size
+        g = lambda i, j: gid[off + local[i, j]]  # noqa: E731
+        i1, j1 = ti[up], tj[up]
+        tris.append(np.stack([g(i1, j1), g(i1 + 1, j1), g(i1, j1 + 1)], 1))
+        i2, j2 = ti[dn], tj[dn]
+        tris.append(np.stack([g(i2 + 1, j2), g(i2 + 1, j2 + 1), g(i2, j2 + 1)], 1))
+    return verts, np.concatenate(tris).astype(np.int64)
+
+
+def uv_sphere(n_tri: int) -> tuple[np.ndarray, np.ndarray]:
+    """Unit latitude/longitude sphere with about n_tri triangles (outward winding):
+    n_lon segments and n_lat rings give 2 * n_lon * (n_lat - 1) triangles."""
+    n_lon = max(8, int(round(np.sqrt(max(n_tri, 32)))))
+    n_lat = max(3, int(round(n_tri / (2.0 * n_lon))) + 1)
+    th = np.pi * np.arange(1, n_lat) / n_lat
+    ph = 2.0 * np.pi * np.arange(n_lon) / n_lon
+    ring = np.stack([np.outer(np.sin(th), np.cos(ph)), np.outer(np.sin(th), np.sin(ph)),
+                     np.outer(np.cos(th), np.ones(n_lon))], -1).reshape(-1, 3)
+    verts = np.vstack([[0.0, 0.0, 1.0], [0.0, 0.0, -1.0], ring])
+    vid = lambda k, j: 2 + (k - 1) * n_lon + (j % n_lon)  # noqa: E731
+    faces = []
+    for j in range(n_lon):
+        faces.append((0, vid(1, j), vid(1, j + 1)))
+        faces.append((1, vid(n_lat - 1, j + 1), vid(n_lat - 1, j)))
+        for k in range(1, n_lat - 1):
+            a, b, c, d = vid(k, j), vid(k, j + 1), vid(k + 1, j), vid(k + 1, j + 1)
+            faces.append((a, c, d))
+            faces.append((a, d, b))
+    return verts, np.asarray(faces, np.int64)
+
+
+def perturbed_sphere(n_tri: int, radius: float, seed: int, **kw) -> MeshArrays:
+    """A geodesic sphere of about n_tri triangles (20 * round(sqrt(n_tri / 20))^2)
+    with the same seeded radial displacement as :func:`perturbed_icosphere`
+    (keyword arguments as there)."""
+    u, f = geodesic_sphere(max(1, int(round(np.sqrt(n_tri / 20.0)))))
+    name = kw.pop("name", None) or f"geo{f.shape[0]}_s{seed}"
+    with_hull = kw.pop("with_hull", True)
+    args = dict(n_harmonics=6, max_degree=3, amplitude=0.15, n_bumps=0, bump_sigma=10.0, bump_height=20.0, scale=1.0)
+    args.update(kw)
+    return _perturbed(u, f, radius, seed, args["n_harmonics"], args["max_degree"], args["amplitude"], args["n_bumps"],
+                      args["bump_sigma"], args["bump_height"], args["scale"], name, with_hull)
+
+
+def _perturbed(u, f, radius, seed, n_harmonics, max_degree, amplitude, n_bumps, bump_sigma, bump_height, scale,
+               name, with_hull) -> MeshArrays:
+    rng = np.random.default_rng(seed)
     theta = np.arccos(np.clip(u[:, 2], -1.0, 1.0))
     phi = np.arctan2(u[:, 1], u[:, 0])
     s = np.zeros(u.shape[0])
@@ -165,7 +245,7 @@ def perturbed_icosphere(subdivisions: int, radius: float, seed: int, n_harmonics
         r = r + h * np.exp(-d2 / (2.0 * bump_sigma ** 2))
     r = np.maximum(r, 0.05 * radius)
     v = (u * r[:, None]) * scale
-    return mesh_from_arrays(v, f, name or f"ico{subdivisions}_s{seed}", with_hull=with_hull, watertight=True)
+    return mesh_from_arrays(v, f, name, with_hull=with_hull, watertight=True)
 
 
 def small_solid(seed: int = 0, with_hull: bool = True) -> MeshArrays:

@@ -1,0 +1,108 @@
+"""Workload suites beyond the single-mesh sweep: many uneven meshes in one
+batched launch, and the learned-proposal search over many meshes.
+
+``batched_suite`` -- seeded meshes with triangle counts log-uniform in
+[t_min, t_max], half from the small-solid generator (r = 50 mm, 1 mm
+voxels, spherical harmonics of degree <= 3, amplitude 0.15) and half from
+the 82k-solid generator (r = 80 mm, 0.5 mm voxels, degree <= 8, amplitude
+0.25, 4 bumps/dents), each on the 1-degree yaw x pitch 0-60 grid.  All
+meshes are swept in one captured graph (``native.Batch``) and, for
+comparison, one by one (``native.Session``); every mesh's results must be
+bit-identical between the two.
+
+``surrogate_suite`` -- small-solid meshes on the 0.5-degree grid
+(yaw 0-359.5 x pitch 0-60, 720 x 121 = 87,120 orientations): the exhaustive
+device sweep against ``surrogate.search`` (5-degree coarse points, 2.5-degree
+proposal blocks).
+
+Both return plain dicts of aggregate figures (times in seconds, device time
+from CUDA events for the sweeps, wall time for the search call).
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from . import meshgen, native, surrogate
+from .options import PrintOptions
+
+
+def uneven_meshes(n: int, seed: int = 0, t_min: int = 1000, t_max: int = 120000):
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n):
+        t = int(round(math.exp(rng.uniform(math.log(t_min), math.log(t_max)))))
+        if k % 2 == 0:
+            m = meshgen.perturbed_sphere(t, 50.0, seed * 1000 + k, with_hull=False)
+        else:
+            m = meshgen.perturbed_sphere(t, 80.0, seed * 1000 + k, n_harmonics=12, max_degree=8, amplitude=0.25,
+                                         n_bumps=4, scale=2.0, with_hull=False)
+        out.append(m)
+    return out
+
+
+def batched_suite(n_meshes: int = 64, seed: int = 0, yaw_step: float = 1.0, pitch_max: float = 60.0,
+                  t_min: int = 1000, t_max: int = 120000) -> dict:
+    meshes = uneven_meshes(n_meshes, seed, t_min, t_max)
+    ypr = meshgen.ypr_grid(np.arange(0, 360, yaw_step), np.arange(0, pitch_max + 1e-9, yaw_step))
+    opts = PrintOptions(explicit_ss=True)
+    plain_s, plain = 0.0, []
+    for m in meshes:
+        s = native.Session(m, ypr, opts)
+        s.run_device()                              # warm (allocations)
+        plain_s += s.run_device() / 1000.0
+        opt, _, mss, _ = s.finish()
+        plain.append((opt, mss.copy(), native.results(ypr.shape[0])["Vss64"].copy()))
+    b = native.Batch(meshes, [ypr] * len(meshes), opts, autotune=True)
+    b.run(use_graph=True)                           # capture + first replay
+    batched_s = b.run(use_graph=True) / 1000.0
+    exact = 0
+    for k, (opt, mss, vss) in enumerate(plain):
+        r = b.results(k)
+        exact += int(r["optID"] == opt and np.array_equal(r["Mss"].view(np.int32), mss.view(np.int32))
+                     and np.array_equal(r["Vss64"], vss))
+    st = native.Batch.stats()
+    native.Batch.release()
+    n_or = len(meshes) * ypr.shape[0]
+    tris = [m.n_tri for m in meshes]
+    return {"meshes": len(meshes), "orientations": n_or, "triangles_min": int(min(tris)),
+            "triangles_max": int(max(tris)), "batched_s": batched_s, "plain_s": plain_s,
+            "batched_orientations_per_s": n_or / batched_s, "plain_orientations_per_s": n_or / plain_s,
+            "batched_triangle_orientations_per_s": sum(tris) * ypr.shape[0] / batched_s,
+            "bit_exact_meshes": exact, "graph_nodes": st["graph_nodes"], "graph_kernels": st["graph_kernels"],
+            "size_classes_tuned": st["tuned_total"], "reruns": st["reruns"]}
+
+
+def surrogate_suite(n_meshes: int = 100, seed0: int = 1000, stride: int = 10, cell: int = 5, top_k: int = 64,
+                    steps: int = 300, ratio_target: float = 0.2, margin: float = 1.0, holdout: float = 0.0,
+                    lr: float = 3e-3, max_eval: int = -1, log_scale: float = 0.3) -> dict:
+    ypr = meshgen.ypr_grid(np.arange(0, 360, 0.5), np.arange(0, 60.5, 0.5))
+    n_yaw, n_pitch = 720, 121
+    opts = PrintOptions(explicit_ss=True)
+    rows = []
+    for k in range(n_meshes):
+        m = meshgen.small_solid(seed0 + k, with_hull=False)
+        s = native.Session(m, ypr, opts)
+        s.run_device()
+        ex_s = s.run_device() / 1000.0
+        opt, _, mss, _ = s.finish()
+        r = surrogate.search(m, ypr, n_yaw, n_pitch, opts, stride=stride, cell=cell, top_k=top_k, steps=steps,
+                             seed=k, margin=margin, holdout=holdout, lr=lr, max_eval=max_eval, log_scale=log_scale)
+        rows.append(dict(same_value=bool(np.float32(r.Mss[r.optID]) == mss[opt]), same_index=r.optID == opt,
+                         ratio=r.seconds / ex_s, exhaustive_s=ex_s, search_s=r.seconds, evaluated=r.evaluated,
+                         fallback=r.fallback, rel_error=r.rel_error))
+    ok = [x["same_value"] and x["ratio"] <= ratio_target for x in rows]
+    return {"meshes": n_meshes, "grid": [n_yaw, n_pitch], "orientations": int(ypr.shape[0]),
+            "coarse_deg": stride * 0.5, "cell_deg": cell * 0.5, "margin": margin, "holdout": holdout,
+            "train_steps": steps, "learning_rate": lr, "max_eval": max_eval, "log_scale": log_scale,
+            "optimum_recall": float(np.mean([x["same_value"] for x in rows])),
+            "same_index": float(np.mean([x["same_index"] for x in rows])),
+            "fallbacks": int(sum(x["fallback"] for x in rows)),
+            "median_time_ratio": float(np.median([x["ratio"] for x in rows])),
+            "p95_time_ratio": float(np.percentile([x["ratio"] for x in rows], 95)),
+            "meshes_at_target": float(np.mean(ok)), "ratio_target": ratio_target,
+            "median_exhaustive_s": float(np.median([x["exhaustive_s"] for x in rows])),
+            "median_search_s": float(np.median([x["search_s"] for x in rows])),
+            "median_evaluated": float(np.median([x["evaluated"] for x in rows])),
+            "median_rel_error": float(np.median([x["rel_error"] for x in rows]))}

@@ -86,15 +86,23 @@ class SearchResult:
     coarse: int
 
 
-def search(mesh, ypr, n_yaw: int, n_pitch: int, opts, cell: int = 10, top_k: int = 8, steps: int = 300,
-           lr: float = 3e-3, seed: int = 0, max_expand: int = 64, gate: float = 0.5) -> SearchResult:
-    """Learned-proposal search over ypr = grid [n_pitch][n_yaw] (yaw fastest)."""
+def search(mesh, ypr, n_yaw: int, n_pitch: int, opts, stride: int = 10, cell: int = 5, top_k: int = 64,
+           steps: int = 300, lr: float = 3e-3, seed: int = 0, max_eval: int = -1, gate: float = 0.5,
+           margin: float = 1.0, holdout: float = 0.0, log_scale: float = 0.3) -> SearchResult:
+    """Learned-proposal search over ypr = grid [n_pitch][n_yaw] (yaw fastest):
+    coarse training points every `stride` grid steps, refinement in blocks of
+    cell x cell grid points, fallback past max_eval evaluated orientations
+    (default: an eighth of the grid); see tomoSurrogateSearch.  The defaults
+    are the setting measured on the 0.5-degree grid with 5-degree coarse
+    points: 64 proposed 2.5-degree blocks, log-scaled targets, margin 1."""
     from .options import pack_info
     f32, i32 = pack_info(opts, mesh, ypr.shape[0])
     ypr, tri, vtx, vn, *_ = _arrays(mesh, ypr)
     n = ypr.shape[0]
-    ip = np.array([cell, top_k, steps, seed, max_expand], np.int32)
-    fp = np.array([lr, gate], np.float32)
+    if max_eval < 0:
+        max_eval = max(1, n // 8)
+    ip = np.array([stride, cell, top_k, steps, seed, max_eval], np.int32)
+    fp = np.array([lr, gate, margin, holdout, log_scale], np.float32)
     mss = np.zeros(n, np.float32)
     pred = np.zeros(n, np.float32)
     st = np.zeros(12, np.float64)
