@@ -172,3 +172,41 @@ def test_bad_index_is_an_error():
     bad.faces[5, 1] = m.n_vtx + 10
     with pytest.raises(native.TomoError):
         native.sweep(bad, GRID_SMALL, PrintOptions())
+
+
+def test_manikin_open_shell(oracle):
+    """The thin open shell workload (87k-triangle manikin union surface with
+    openings and a 2 mm inward wall, shell mode, a ~1000-column slot grid) on
+    a few orientations of its 1-degree grid."""
+    m = meshgen.manikin_shell(0)
+    ypr = np.ascontiguousarray(meshgen.ypr_grid(np.arange(0, 360, 1), np.arange(0, 61, 1))[::3989])
+    opts = PrintOptions(explicit_ss=True, shell_mesh=True, shell_thickness=0.5)
+    res = native.sweep(m, ypr, opts)
+    G = native.stats()["grid"]
+    assert G > 256
+    _compare(res, oracle.sweep(m, ypr, opts, grid=G, threads=2), "manikin")
+
+
+@pytest.mark.parametrize("adaptive", [0, 1])
+def test_overflow_ladder_and_adaptive_budget(oracle, adaptive):
+    """A strip budget far too small for the mesh: with adaptation off every
+    orientation overflows and is re-run with the large budget; with it on,
+    the sweep raises its budget after the first batches.  Both exact."""
+    m = meshgen.perturbed_icosphere(5, 60.0, 31, with_hull=False)
+    ypr = meshgen.ypr_grid(np.arange(0, 360, 15), np.arange(0, 70, 10))
+    opts = PrintOptions()
+    native.set_option(native.TOMO_OPT_ADAPTIVE, adaptive)
+    native.set_option(native.TOMO_OPT_NORMAL_SMEM, 24576)
+    native.set_option(native.TOMO_OPT_BATCH, 32)
+    try:
+        res = native.sweep(m, ypr, opts)
+        st = native.stats()
+    finally:
+        native.set_option(native.TOMO_OPT_ADAPTIVE, 1)
+        native.set_option(native.TOMO_OPT_NORMAL_SMEM, 0)
+        native.set_option(native.TOMO_OPT_BATCH, 128)
+    _compare(res, oracle.sweep(m, ypr, opts), f"adaptive={adaptive}")
+    if adaptive:
+        assert st["overflow_reruns"] < ypr.shape[0] // 2
+    else:
+        assert st["overflow_reruns"] > 0

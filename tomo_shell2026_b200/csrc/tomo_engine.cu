@@ -313,6 +313,8 @@ struct Engine {
   int force_safe = 0;     // test hook: run every orientation in safe mode
   int normal_smem = 0;    // shared-memory budget of a normal strip CTA (0 = 72 KB)
   int export_pixels = 1;  // rebuild the best orientation's pixels and vm_info (TomoSh_CUDA tail)
+  int adaptive = 1;       // raise the entry budget after overflowing early batches (full sweeps)
+  int adapt_smem = 0, adapt_h = 0;   // configuration adapted to by an earlier sweep of this upload
   float cx = 0, cy = 0, cz = 0;
   std::vector<float> h_rot;
   std::vector<long long> vo64, vss64, vtc64, entries, columns;
@@ -423,6 +425,7 @@ struct Engine {
         P.bed_outer > 1000.f)
       return set_error(TOMO_ERR_ARG, "bad printer parameters");
     nYPR = P.n_ypr;
+    adapt_smem = adapt_h = 0;
     // AABB centre of the raw vertices (STomoAABB3Df.cpp:58-72)
     float mn[3] = {1e5f, 1e5f, 1e5f}, mx[3] = {-1e5f, -1e5f, -1e5f};
     for (int v = 0; v < P.n_vtx; v++)
@@ -537,6 +540,52 @@ struct Engine {
   {
     const int n = ids ? n_ids : nYPR;
     if (n == 0 || P.n_tri == 0) return 0;
+    // a full sweep starts from the configuration an earlier sweep of this
+    // upload adapted to (see adapt_after below)
+    const int user_smem = normal_smem, user_h = force_h;
+    const bool adapt = adaptive && !ids;
+    if (adapt && adapt_smem) { normal_smem = adapt_smem; force_h = adapt_h; plan_strips(); }
+    const int rc = sweep_batches(ids, n, adapt);
+    if (adapt && (normal_smem != user_smem || force_h != user_h)) {
+      normal_smem = user_smem; force_h = user_h; plan_strips();
+    }
+    return rc;
+  }
+
+  // After an early batch: if more than a fifth of its orientations overflowed
+  // their strip lists, give the rest of the sweep the next larger entry
+  // budget at the same strip height (one host wait per check; the overflowed
+  // orientations are re-run by the ladder as usual).  Returns true when the
+  // configuration changed.
+  int adapt_after(int first, int nb, bool* changed)
+  {
+    *changed = false;
+    static const int kBudgets[] = {73728, 101376, 150528, 0};   // 0: everything the SM allows
+    const size_t cur = cfg[0].smem;
+    int next = -1;
+    for (int b : kBudgets) {
+      const size_t lim = b ? (size_t)b : (size_t)std::min<size_t>(smem_optin, 227 * 1024) - 2048;
+      if (lim > cur + 4096) { next = b ? b : (int)lim; break; }
+    }
+    if (next < 0) return 0;
+    std::vector<int> fl(nb);
+    TOMO_CUDA(cudaStreamSynchronize(side));
+    TOMO_CUDA(cudaMemcpy(fl.data(), o_flags.ptr + first, sizeof(int) * nb, cudaMemcpyDeviceToHost));
+    int over = 0;
+    for (int f : fl) over += (f & kFlagOverflow) ? 1 : 0;
+    if (over * 5 <= nb) return 0;
+    force_h = H;
+    normal_smem = next;
+    plan_strips();
+    choose_strips(0);
+    TOMO_TRY(configure());
+    adapt_smem = normal_smem; adapt_h = force_h;
+    *changed = true;
+    return 0;
+  }
+
+  int sweep_batches(const int* ids, int n, bool adapt)
+  {
     choose_strips(0);
     H_sweep = H;
     TOMO_TRY(configure());
@@ -559,6 +608,11 @@ struct Engine {
       TOMO_CUDA(cudaStreamWaitEvent(side, ev_ready, 0));
       TOMO_CUDA(launch_fold(p, side, &log));
       TOMO_CUDA(cudaEventRecord(set[which].folded, side));
+      if (adapt && k < 3 && first + nb < n) {
+        bool changed = false;
+        TOMO_TRY(adapt_after(first, nb, &changed));
+        if (changed) p = base_params(0);
+      }
     }
     // join the side stream back into main
     TOMO_CUDA(cudaEventRecord(ev_ready, side));
@@ -1218,6 +1272,7 @@ int tomoSetOption(int key, int value)
     case TOMO_OPT_FORCE_SAFE: E.force_safe = value ? 1 : 0; return 0;
     case TOMO_OPT_NORMAL_SMEM: if (value < 0 || value > 232448) return TOMO_ERR_ARG; E.normal_smem = value; return 0;
     case TOMO_OPT_EXPORT: E.export_pixels = value ? 1 : 0; return 0;
+    case TOMO_OPT_ADAPTIVE: E.adaptive = value ? 1 : 0; E.adapt_smem = E.adapt_h = 0; return 0;
     default: return TOMO_ERR_ARG;
   }
 }
@@ -1693,6 +1748,7 @@ struct MultiEngine {
       if (f32 == nullptr || i32 == nullptr || f32[m] == nullptr || i32[m] == nullptr)
         return set_error(TOMO_ERR_ARG, "mesh " + std::to_string(m) + ": info arrays are null");
       Engine* e = new Engine(W);
+      e->adaptive = 0;   // captured into a graph: no host waits inside the sweep
       meshes.push_back(e);
       const int rc = e->upload(f32[m], i32[m], ypr ? ypr[m] : nullptr, tri ? tri[m] : nullptr, vtx ? vtx[m] : nullptr,
                                vnrm ? vnrm[m] : nullptr);

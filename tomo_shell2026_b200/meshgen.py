@@ -285,3 +285,116 @@ def ypr_grid(yaw_deg, pitch_deg, roll_deg=(0.0,)) -> np.ndarray:
     roll = np.asarray(roll_deg, np.float64) * np.pi / 180.0
     xx, yy, zz = np.meshgrid(yaw.astype(np.float32), pitch.astype(np.float32), roll.astype(np.float32))
     return np.ascontiguousarray(np.column_stack([xx.ravel(), yy.ravel(), zz.ravel()]).astype(np.float32))
+
+
+# ------------------------------------------------------------------ thin open shell
+
+def _surface_nets(f: np.ndarray, origin: np.ndarray, h: float) -> tuple[np.ndarray, np.ndarray]:
+    """Triangulate the zero level set of a sampled signed distance f[nx, ny, nz]
+    (negative inside) by surface nets: one vertex per sign-changing cube at
+    the mean of its edge crossings, one quad (two triangles) per
+    sign-changing grid edge, wound so normals point to the positive side."""
+    nx, ny, nz = f.shape
+    inside = f < 0
+    # cube index of every sign-changing cube
+    corners = [inside[a:nx - 1 + a, b:ny - 1 + b, c:nz - 1 + c] for a in (0, 1) for b in (0, 1) for c in (0, 1)]
+    anyin = np.logical_or.reduce(corners)
+    allin = np.logical_and.reduce(corners)
+    active = anyin & ~allin
+    cid = -np.ones(active.shape, np.int64)
+    cid[active] = np.arange(int(active.sum()))
+    # vertex positions: mean of crossings on the cube's 12 edges
+    acc = np.zeros(active.shape + (3,))
+    cnt = np.zeros(active.shape)
+    offs = [(0, 0, 0), (1, 0, 0), (0, 1, 0), (0, 0, 1), (1, 1, 0), (1, 0, 1), (0, 1, 1), (1, 1, 1)]
+    edges = [(0, 1), (0, 2), (0, 3), (1, 4), (1, 5), (2, 4), (2, 6), (3, 5), (3, 6), (4, 7), (5, 7), (6, 7)]
+    sl = lambda o: (slice(o[0], nx - 1 + o[0]), slice(o[1], ny - 1 + o[1]), slice(o[2], nz - 1 + o[2]))  # noqa: E731
+    for a, b in edges:
+        fa, fb = f[sl(offs[a])], f[sl(offs[b])]
+        cross = (fa < 0) != (fb < 0)
+        t = np.where(cross, fa / np.where(cross, fa - fb, 1.0), 0.0)
+        pa, pb = np.array(offs[a], float), np.array(offs[b], float)
+        pos = pa[None, None, None, :] + t[..., None] * (pb - pa)[None, None, None, :]
+        acc += np.where(cross[..., None], pos, 0.0)
+        cnt += cross
+    ii, jj, kk = np.nonzero(active)
+    local = acc[active] / cnt[active][:, None]
+    verts = origin[None, :] + (np.stack([ii, jj, kk], 1) + local) * h
+    faces = []
+    # an x-edge (i, j, k)-(i+1, j, k) is shared by cubes (i, j-1..j, k-1..k)
+    for axis in range(3):
+        a0 = [slice(0, n - 1) if d == axis else slice(1, n - 1) for d, n in enumerate(f.shape)]
+        a1 = [slice(1, n) if d == axis else slice(1, n - 1) for d, n in enumerate(f.shape)]
+        s0, s1 = inside[tuple(a0)], inside[tuple(a1)]
+        change = s0 != s1
+        e = np.nonzero(change)
+        base = [e[d] + (0 if d == axis else 1) for d in range(3)]
+        u, v = [d for d in range(3) if d != axis]
+
+        def cube(du, dv):
+            idx = list(base)
+            idx[u] = idx[u] - du
+            idx[v] = idx[v] - dv
+            return cid[idx[0], idx[1], idx[2]]
+
+        c00, c10, c11, c01 = cube(1, 1), cube(0, 1), cube(0, 0), cube(1, 0)
+        # (c00, c10, c11, c01) turns counter-clockwise in the (u, v) plane: its
+        # normal is +axis when (u, v, axis) is right-handed (axes x and z), -axis
+        # for y; the normal must point to the outside (positive) end of the edge
+        plus = s0[e]   # inside at the low end: outside along +axis
+        flip = ~plus if axis != 1 else plus
+        q = np.stack([c00, c10, c11, c01], 1)
+        q[flip] = q[flip][:, ::-1]
+        ok = (q >= 0).all(1)
+        q = q[ok]
+        faces.append(np.concatenate([q[:, [0, 1, 2]], q[:, [0, 2, 3]]]))
+    return verts, np.concatenate(faces)
+
+
+def manikin_shell(seed: int = 0, spacing: float = 6.5, offset: float = 2.0, with_hull: bool = False) -> MeshArrays:
+    """Thin open shell, manikin-like: the union surface of 9 seeded
+    ellipsoids and capsules (torso ~300 x 200 x 600 mm, hips, chest, neck,
+    head, upper and lower arms) triangulated by surface nets at `spacing` mm,
+    the bottom and both arm ends cut open, plus an inward copy offset by
+    `offset` mm along the vertex normals with reversed winding (the wall).
+    spacing 6.5 mm gives ~87k triangles for both sheets together."""
+    rng = np.random.default_rng(seed)
+    j = lambda s: 1.0 + rng.uniform(-s, s)  # noqa: E731
+    ell = [((0, 0, 330), (150 * j(.05), 100 * j(.05), 230 * j(.05))),      # torso
+           ((0, 0, 150), (160 * j(.05), 110 * j(.05), 120 * j(.05))),      # hips
+           ((0, 15, 430), (140 * j(.05), 95 * j(.05), 90 * j(.05))),       # chest
+           ((0, 0, 690), (70 * j(.05), 80 * j(.05), 100 * j(.05)))]        # head
+    cap = [((0, 0, 540), (0, 0, 610), 45 * j(.05)),                         # neck
+           ((-150, 0, 510), (-250, 0, 330), 45 * j(.05)), ((150, 0, 510), (250, 0, 330), 45 * j(.05)),
+           ((-250, 0, 330), (-290, 30, 160), 38 * j(.05)), ((250, 0, 330), (290, 30, 160), 38 * j(.05))]
+    lo = np.array([-360.0, -160.0, 0.0])
+    hi = np.array([360.0, 160.0, 820.0])
+    n = np.ceil((hi - lo) / spacing).astype(int) + 1
+    X, Y, Z = np.meshgrid(*[lo[d] + spacing * np.arange(n[d]) for d in range(3)], indexing="ij")
+    P = np.stack([X, Y, Z], -1)
+    f = np.full(X.shape, np.inf)
+    for c, r in ell:
+        q = (P - np.array(c)) / np.array(r)
+        f = np.minimum(f, (np.linalg.norm(q, axis=-1) - 1.0) * min(r))
+    for a, b, r in cap:
+        a, b = np.array(a, float), np.array(b, float)
+        ab = b - a
+        t = np.clip(((P - a) @ ab) / (ab @ ab), 0.0, 1.0)
+        f = np.minimum(f, np.linalg.norm(P - (a + t[..., None] * ab), axis=-1) - r)
+    v, tri = _surface_nets(f, lo, spacing)
+    cen = v[tri].mean(1)
+    keep = cen[:, 2] > 70.0                                               # bottom opening
+    for a, b, _ in cap[3:]:
+        a, b = np.array(a, float), np.array(b, float)
+        axis = (b - a) / np.linalg.norm(b - a)
+        keep &= ((cen - b) @ axis) < -10.0                                # arm openings at the hands
+    tri = tri[keep]
+    used = np.unique(tri)
+    remap = -np.ones(v.shape[0], np.int64)
+    remap[used] = np.arange(used.size)
+    v, tri = v[used], remap[tri]
+    vn, _, _ = _normals(v.astype(np.float32), tri.astype(np.int32))
+    inner = v - offset * vn.astype(np.float64)
+    V = np.vstack([v, inner])
+    F = np.vstack([tri, tri[:, ::-1] + v.shape[0]])
+    return mesh_from_arrays(V, F, f"manikin_s{seed}", with_hull=with_hull)

@@ -74,6 +74,38 @@ def batched_suite(n_meshes: int = 64, seed: int = 0, yaw_step: float = 1.0, pitc
             "size_classes_tuned": st["tuned_total"], "reruns": st["reruns"]}
 
 
+def block_rank(score: np.ndarray, target: int, n_yaw: int, n_pitch: int, cell: int) -> int:
+    """Rank (0 = first) of the block holding grid point `target` when blocks
+    are ordered by their smallest score."""
+    ncy = (n_yaw + cell - 1) // cell
+    ids = np.arange(score.size)
+    blk = (ids % n_yaw) // cell + ((ids // n_yaw) // cell) * ncy
+    bmin = np.full(blk.max() + 1, np.inf)
+    np.minimum.at(bmin, blk, score)
+    order = np.argsort(bmin, kind="stable")
+    return int(np.nonzero(order == blk[target])[0][0])
+
+
+def coarse_interpolation(vss: np.ndarray, n_yaw: int, n_pitch: int, stride: int) -> np.ndarray:
+    """The method without the network: exact Vss of the coarse points,
+    bilinearly interpolated onto the grid (yaw periodic)."""
+    g = vss.reshape(n_pitch, n_yaw).astype(np.float64)
+    cy = np.arange(0, n_yaw, stride)
+    cp = np.arange(0, n_pitch, stride)
+    c = g[np.ix_(cp, cy)]
+    fy = np.arange(n_yaw) / stride
+    fp = np.minimum(np.arange(n_pitch) / stride, len(cp) - 1)
+    y0 = np.floor(fy).astype(int) % len(cy)
+    y1 = (y0 + 1) % len(cy)
+    wy = fy - np.floor(fy)
+    p0 = np.floor(fp).astype(int)
+    p1 = np.minimum(p0 + 1, len(cp) - 1)
+    wp = fp - p0
+    rows = c[p0][:, y0] * (1 - wy) + c[p0][:, y1] * wy
+    rows1 = c[p1][:, y0] * (1 - wy) + c[p1][:, y1] * wy
+    return ((1 - wp)[:, None] * rows + wp[:, None] * rows1).ravel()
+
+
 def surrogate_suite(n_meshes: int = 100, seed0: int = 1000, stride: int = 10, cell: int = 5, top_k: int = 64,
                     steps: int = 300, ratio_target: float = 0.2, margin: float = 1.0, holdout: float = 0.0,
                     lr: float = 3e-3, max_eval: int = -1, log_scale: float = 0.3) -> dict:
@@ -87,11 +119,15 @@ def surrogate_suite(n_meshes: int = 100, seed0: int = 1000, stride: int = 10, ce
         s.run_device()
         ex_s = s.run_device() / 1000.0
         opt, _, mss, _ = s.finish()
+        vss = native.results(ypr.shape[0])["Vss64"]
         r = surrogate.search(m, ypr, n_yaw, n_pitch, opts, stride=stride, cell=cell, top_k=top_k, steps=steps,
                              seed=k, margin=margin, holdout=holdout, lr=lr, max_eval=max_eval, log_scale=log_scale)
         rows.append(dict(same_value=bool(np.float32(r.Mss[r.optID]) == mss[opt]), same_index=r.optID == opt,
                          ratio=r.seconds / ex_s, exhaustive_s=ex_s, search_s=r.seconds, evaluated=r.evaluated,
-                         fallback=r.fallback, rel_error=r.rel_error))
+                         fallback=r.fallback, rel_error=r.rel_error,
+                         rank_network=block_rank(r.pred_vss, opt, n_yaw, n_pitch, cell),
+                         rank_without=block_rank(coarse_interpolation(vss, n_yaw, n_pitch, stride), opt, n_yaw,
+                                                 n_pitch, cell)))
     ok = [x["same_value"] and x["ratio"] <= ratio_target for x in rows]
     return {"meshes": n_meshes, "grid": [n_yaw, n_pitch], "orientations": int(ypr.shape[0]),
             "coarse_deg": stride * 0.5, "cell_deg": cell * 0.5, "margin": margin, "holdout": holdout,
@@ -105,4 +141,10 @@ def surrogate_suite(n_meshes: int = 100, seed0: int = 1000, stride: int = 10, ce
             "median_exhaustive_s": float(np.median([x["exhaustive_s"] for x in rows])),
             "median_search_s": float(np.median([x["search_s"] for x in rows])),
             "median_evaluated": float(np.median([x["evaluated"] for x in rows])),
-            "median_rel_error": float(np.median([x["rel_error"] for x in rows]))}
+            "median_rel_error": float(np.median([x["rel_error"] for x in rows])),
+            # where the optimum's block lands when blocks are ranked by the
+            # network versus by interpolating the exact coarse values
+            "optimum_block_in_top_k_network": float(np.mean([x["rank_network"] < top_k for x in rows])),
+            "optimum_block_in_top_k_without_network": float(np.mean([x["rank_without"] < top_k for x in rows])),
+            "median_optimum_block_rank_network": float(np.median([x["rank_network"] for x in rows])),
+            "median_optimum_block_rank_without_network": float(np.median([x["rank_without"] for x in rows]))}
