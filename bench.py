@@ -323,6 +323,7 @@ def run_ours(args, rank, world, local_rank):
         from tomo_shell2026_b200 import suites
         line["batched"] = suites.batched_suite(n_meshes=args.batched_meshes)
         line["surrogate"] = suites.surrogate_suite(n_meshes=args.surrogate_meshes)
+        line["shell"] = suites.shell_suite()
     if rank == 0:
         print(json.dumps(line), flush=True)
     return 0
@@ -354,6 +355,10 @@ def run_suite(args) -> int:
         line = {"metric": "aggregate orientations/s, 64 uneven meshes (1k-120k tris), 1deg grid, one graph launch",
                 "value": r["batched_orientations_per_s"], "unit": "orientations/s", "higher_is_better": True,
                 "suite": r}
+    elif args.suite == "shell":
+        r = suites.shell_suite()
+        line = {"metric": "orientations/s, 87k-tri thin open shell (manikin-like, 2 mm wall), 1deg grid, shell mode",
+                "value": r["orientations_per_s"], "unit": "orientations/s", "higher_is_better": True, "suite": r}
     else:
         r = suites.surrogate_suite(n_meshes=100)
         line = {"metric": "learned-proposal search: meshes reaching the exhaustive optimum in <= 1/5 of its time",
@@ -408,7 +413,7 @@ def main():
                     help="skip the plain-launch, batched and surrogate figures added to the line")
     ap.add_argument("--batched-meshes", type=int, default=16)
     ap.add_argument("--surrogate-meshes", type=int, default=10)
-    ap.add_argument("--suite", choices=("none", "batched", "surrogate"), default="none",
+    ap.add_argument("--suite", choices=("none", "batched", "surrogate", "shell"), default="none",
                     help="run a full-size suite instead (64 uneven meshes / 100 searched meshes)")
     ap.add_argument("--max-orientations", type=int, default=0,
                     help="keep only the first N orientations (small profiling cases; 0 = the whole grid)")

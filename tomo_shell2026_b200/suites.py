@@ -15,7 +15,11 @@ bit-identical between the two.
 device sweep against ``surrogate.search`` (5-degree coarse points, 2.5-degree
 proposal blocks).
 
-Both return plain dicts of aggregate figures (times in seconds, device time
+``shell_suite`` -- the thin open shell (manikin-like union surface, openings,
+2 mm inward wall; shell mode, 1 mm voxels) on the 1-degree yaw x pitch 0-60
+grid: device orientations/s of the full sweep.
+
+All return plain dicts of aggregate figures (times in seconds, device time
 from CUDA events for the sweeps, wall time for the search call).
 """
 from __future__ import annotations
@@ -148,3 +152,20 @@ def surrogate_suite(n_meshes: int = 100, seed0: int = 1000, stride: int = 10, ce
             "optimum_block_in_top_k_without_network": float(np.mean([x["rank_without"] < top_k for x in rows])),
             "median_optimum_block_rank_network": float(np.median([x["rank_network"] for x in rows])),
             "median_optimum_block_rank_without_network": float(np.median([x["rank_without"] for x in rows]))}
+
+
+def shell_suite(seed: int = 0) -> dict:
+    m = meshgen.manikin_shell(seed)
+    ypr = meshgen.ypr_grid(np.arange(0, 360), np.arange(0, 61))
+    opts = PrintOptions(explicit_ss=True, shell_mesh=True, shell_thickness=0.5)
+    s = native.Session(m, ypr, opts)
+    s.run_device()
+    sec = s.run_device() / 1000.0
+    opt, _, _, _ = s.finish()
+    st = native.stats()
+    r = native.results(ypr.shape[0])
+    return {"mesh": "manikin-like open shell, union of 9 ellipsoids/capsules, 2 mm wall", "triangles": m.n_tri,
+            "orientations": int(ypr.shape[0]), "seconds": sec, "orientations_per_s": ypr.shape[0] / sec,
+            "triangle_orientations_per_s": m.n_tri * ypr.shape[0] / sec, "slot_grid": st["grid"],
+            "strip_h": st["strip_h"], "entries_per_orientation": float(r["entries"].mean()),
+            "overflow_reruns": st["overflow_reruns"], "safe_reruns": st["safe_reruns"], "optID": int(opt)}
