@@ -94,8 +94,9 @@ void tomoVolToMass(const float* f32info, const int* i32info, float* vm22);
 #define TOMO_OPT_ADAPTIVE 6     /* 0 = keep the planned strip budget even when early batches overflow (default 1) */
 int tomoSetOption(int key, int value);
 
-/* out[0..7] = grid edge, strip height, strips, entry capacity, orientations re-run
- * with a large strip capacity, nYPR, batch, orientations re-run in safe mode */
+/* out[0..8] = grid edge, strip height, strips, entry capacity, orientations re-run
+ * with a large strip capacity, nYPR, batch, orientations re-run in safe mode,
+ * orientations re-run with first-come priorities (a column past the 63 cap) */
 int tomoGetStats(long long* out, int n);
 
 /* Per-orientation results of the last sweep; any pointer may be null. */

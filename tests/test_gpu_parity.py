@@ -210,3 +210,16 @@ def test_overflow_ladder_and_adaptive_budget(oracle, adaptive):
         assert st["overflow_reruns"] < ypr.shape[0] // 2
     else:
         assert st["overflow_reruns"] > 0
+
+
+def test_dense_mesh_first_come_priorities(oracle):
+    """A 100k-triangle solid at 1 mm: columns along the silhouette pass the
+    63-pixel cap, so which keys survive depends on first-come order; those
+    orientations are re-run with priorities carried in the normal strips."""
+    m = meshgen.perturbed_sphere(100000, 50.0, 7, with_hull=False)
+    ypr = meshgen.ypr_grid(np.arange(0, 360, 45), np.arange(0, 61, 30))
+    opts = PrintOptions()
+    res = native.sweep(m, ypr, opts)
+    st = native.stats()
+    _compare(res, oracle.sweep(m, ypr, opts), "dense")
+    assert st["prio_reruns"] > 0

@@ -33,7 +33,10 @@ enum : int {
   kFlagBinCap = 4,     // triangle bin list exceeded its capacity
   kFlagGrid = 8,       // a slot index fell outside the grid (grid too small)
   kFlagSafeOverflow = 16,
+  kFlagCap = 32,       // a column exceeded the 63-pixel cap: needs first-come priorities
 };
+// Results of an orientation flagged with any of these are not written.
+constexpr int kFlagRedo = kFlagStray | kFlagOverflow | kFlagBinCap | kFlagCap;
 
 // Bed bookkeeping per slot (GenerateBed / IsBedCandidate, STomoSh_INT3.cpp:1331-1443).
 enum : uint8_t {
@@ -70,7 +73,7 @@ struct EngineParams {
   int G;                // square grid edge; slot id = x * G + y
   int H;                // strip height in x columns
   int S;                // number of strips = ceil(G / H)
-  int mode;             // 0 normal, 1 safe
+  int mode;             // 0 normal, 1 safe, 2 normal with priorities
   int variant;          // strip configuration (launch accounting only)
 
   // raster constants

@@ -30,7 +30,7 @@
 namespace tomo {
 
 size_t strip_smem_bytes(int mode, int H, int G, int ent_cap);
-cudaError_t configure_kernels(size_t normal_smem, size_t safe_smem);
+cudaError_t configure_kernels(size_t normal_smem, size_t safe_smem, size_t prio_smem);
 cudaError_t launch_batch(const EngineParams& p, cudaStream_t main, size_t strip_smem, LaunchLog* L);
 cudaError_t launch_fold(const EngineParams& p, cudaStream_t side, LaunchLog* L);
 cudaError_t launch_bin_count(const EngineParams& p, cudaStream_t main, LaunchLog* L);
@@ -315,6 +315,7 @@ struct Engine {
   int export_pixels = 1;  // rebuild the best orientation's pixels and vm_info (TomoSh_CUDA tail)
   int adaptive = 1;       // raise the entry budget after overflowing early batches (full sweeps)
   int adapt_smem = 0, adapt_h = 0;   // configuration adapted to by an earlier sweep of this upload
+  int adapt_cfg = 0;                  // 4 once a sweep of this upload switched to priority strips
   float cx = 0, cy = 0, cz = 0;
   std::vector<float> h_rot;
   std::vector<long long> vo64, vss64, vtc64, entries, columns;
@@ -324,7 +325,7 @@ struct Engine {
   float mat4x4[16] = {0};
   double last_kernel_ms = 0.0;
   int n_safe = 0;
-  int n_redo[4] = {0, 0, 0, 0};
+  int n_redo[5] = {0, 0, 0, 0, 0};
   int H_sweep = 0;        // strip height of the last normal sweep
 
   int init() { return W.init(); }
@@ -363,9 +364,12 @@ struct Engine {
   //                  all opt-in shared memory;
   //   2 big normal : configuration 0 semantics with all opt-in shared memory
   //                  (orientations whose strip lists overflowed);
-  //   3 narrow safe: safe mode with one-column strips (last resort).
+  //   3 narrow safe: safe mode with one-column strips (last resort);
+  //   4 priorities : configuration 0 strips whose entries also carry their
+  //                  first-come priority, all opt-in shared memory, for
+  //                  orientations where a column passed the 63-pixel cap.
   struct StripCfg { int H, S, C; size_t smem; int mode; };
-  StripCfg cfg[4];
+  StripCfg cfg[5];
 
   void plan_strips()
   {
@@ -394,6 +398,7 @@ struct Engine {
     cfg[1] = make(1, h0, budget1);
     cfg[2] = make(0, h0, budget1);
     cfg[3] = make(1, 1, budget1);
+    cfg[4] = make(2, h0, budget1);
   }
 
   void choose_strips(int c)
@@ -403,7 +408,7 @@ struct Engine {
 
   int configure()
   {
-    TOMO_CUDA(configure_kernels(std::max(cfg[0].smem, cfg[2].smem), std::max(cfg[1].smem, cfg[3].smem)));
+    TOMO_CUDA(configure_kernels(std::max(cfg[0].smem, cfg[2].smem), std::max(cfg[1].smem, cfg[3].smem), cfg[4].smem));
     return 0;
   }
 
@@ -425,7 +430,7 @@ struct Engine {
         P.bed_outer > 1000.f)
       return set_error(TOMO_ERR_ARG, "bad printer parameters");
     nYPR = P.n_ypr;
-    adapt_smem = adapt_h = 0;
+    adapt_smem = adapt_h = adapt_cfg = 0;
     // AABB centre of the raw vertices (STomoAABB3Df.cpp:58-72)
     float mn[3] = {1e5f, 1e5f, 1e5f}, mx[3] = {-1e5f, -1e5f, -1e5f};
     for (int v = 0; v < P.n_vtx; v++)
@@ -557,36 +562,48 @@ struct Engine {
   // budget at the same strip height (one host wait per check; the overflowed
   // orientations are re-run by the ladder as usual).  Returns true when the
   // configuration changed.
-  int adapt_after(int first, int nb, bool* changed)
+  // A batch where most orientations passed the 63-pixel cap in some column
+  // switches the rest of the sweep to the priority-carrying strips
+  // (configuration 4), which resolve those columns in one pass.
+  int adapt_after(int first, int nb, int* c, bool* changed)
   {
     *changed = false;
     static const int kBudgets[] = {73728, 101376, 150528, 0};   // 0: everything the SM allows
-    const size_t cur = cfg[0].smem;
     int next = -1;
-    for (int b : kBudgets) {
-      const size_t lim = b ? (size_t)b : (size_t)std::min<size_t>(smem_optin, 227 * 1024) - 2048;
-      if (lim > cur + 4096) { next = b ? b : (int)lim; break; }
+    if (*c == 0) {
+      const size_t cur = cfg[0].smem;
+      for (int b : kBudgets) {
+        const size_t lim = b ? (size_t)b : (size_t)std::min<size_t>(smem_optin, 227 * 1024) - 2048;
+        if (lim > cur + 4096) { next = b ? b : (int)lim; break; }
+      }
     }
-    if (next < 0) return 0;
+    if (*c != 0) return 0;
     std::vector<int> fl(nb);
     TOMO_CUDA(cudaStreamSynchronize(side));
     TOMO_CUDA(cudaMemcpy(fl.data(), o_flags.ptr + first, sizeof(int) * nb, cudaMemcpyDeviceToHost));
-    int over = 0;
-    for (int f : fl) over += (f & kFlagOverflow) ? 1 : 0;
-    if (over * 5 <= nb) return 0;
-    force_h = H;
-    normal_smem = next;
-    plan_strips();
-    choose_strips(0);
+    int over = 0, cap = 0;
+    for (int f : fl) { over += (f & kFlagOverflow) ? 1 : 0; cap += (f & kFlagCap) ? 1 : 0; }
+    if (cap * 2 > nb) {
+      *c = 4;
+      adapt_cfg = 4;
+    } else if (next >= 0 && over * 5 > nb) {
+      force_h = H;
+      normal_smem = next;
+      plan_strips();
+      adapt_smem = normal_smem; adapt_h = force_h;
+    } else {
+      return 0;
+    }
+    choose_strips(*c);
     TOMO_TRY(configure());
-    adapt_smem = normal_smem; adapt_h = force_h;
     *changed = true;
     return 0;
   }
 
   int sweep_batches(const int* ids, int n, bool adapt)
   {
-    choose_strips(0);
+    int c = (adapt && adapt_cfg == 4) ? 4 : 0;
+    choose_strips(c);
     H_sweep = H;
     TOMO_TRY(configure());
     const int Bo = std::min(batch, n);
@@ -595,7 +612,7 @@ struct Engine {
     TOMO_TRY(reserve_batch(Bo, bin_cap));
     if (ids) TOMO_CUDA(launch_zero_ids(o_nbed.ptr, ids, n, main));
     else TOMO_CUDA(cudaMemsetAsync(o_nbed.ptr, 0, sizeof(int) * nYPR, main));
-    EngineParams p = base_params(0);
+    EngineParams p = base_params(cfg[c].mode);
     int k = 0;
     for (int first = 0; first < n; first += Bo, k++) {
       const int nb = std::min(Bo, n - first);
@@ -603,15 +620,15 @@ struct Engine {
       if (k >= 2) TOMO_CUDA(cudaStreamWaitEvent(main, set[which].folded, 0));
       bind_batch(p, nb, bin_cap, which, first);
       if (ids) p.ori = ids + first;
-      TOMO_CUDA(launch_batch(p, main, cfg[0].smem, &log));
+      TOMO_CUDA(launch_batch(p, main, cfg[c].smem, &log));
       TOMO_CUDA(cudaEventRecord(ev_ready, main));
       TOMO_CUDA(cudaStreamWaitEvent(side, ev_ready, 0));
       TOMO_CUDA(launch_fold(p, side, &log));
       TOMO_CUDA(cudaEventRecord(set[which].folded, side));
       if (adapt && k < 3 && first + nb < n) {
         bool changed = false;
-        TOMO_TRY(adapt_after(first, nb, &changed));
-        if (changed) p = base_params(0);
+        TOMO_TRY(adapt_after(first, nb, &c, &changed));
+        if (changed) p = base_params(cfg[c].mode);
       }
     }
     // join the side stream back into main
@@ -634,13 +651,13 @@ struct Engine {
     TOMO_CUDA(cudaMemcpyAsync(sub.ptr, ids.data(), sizeof(int) * ids.size(), cudaMemcpyHostToDevice, main));
     const int Bo = std::min<int>(batch, (int)ids.size());
     const int normal_cap = 4 * P.n_tri + 4096;
-    TOMO_TRY(reserve_batch(Bo, mode == 0 ? normal_cap : 1));
+    TOMO_TRY(reserve_batch(Bo, mode != 1 ? normal_cap : 1));
     EngineParams p = base_params(mode);
     p.variant = c;
     for (int first = 0; first < (int)ids.size(); first += Bo) {
       const int nb = std::min<int>(Bo, (int)ids.size() - first);
       for (int o = 0; o < nb; o++) TOMO_CUDA(cudaMemsetAsync(o_nbed.ptr + ids[first + o], 0, sizeof(int), main));
-      if (mode == 0) {
+      if (mode != 1) {
         bind_batch(p, nb, normal_cap, 0, 0);
         p.ori = sub.ptr + first;
         TOMO_CUDA(launch_batch(p, main, cfg[c].smem, &log));
@@ -779,7 +796,7 @@ struct Engine {
   int resolve_ids(const std::vector<int>& ids)
   {
     const std::vector<int>* subset = &ids;
-    std::vector<int> big, safe, narrow;
+    std::vector<int> big, prio, safe, narrow;
     if (force_safe) {
       if (nYPR == 0 || P.n_tri == 0) return fetch();
       TOMO_TRY(reserve_outputs());
@@ -790,12 +807,21 @@ struct Engine {
         if (flags[i] & kFlagGrid) return set_error(TOMO_ERR_CAPACITY, "slot index outside the grid");
         if (flags[i] & (kFlagStray | kFlagBinCap)) safe.push_back(i);
         else if (flags[i] & kFlagOverflow) big.push_back(i);
+        else if (flags[i] & kFlagCap) prio.push_back(i);
       }
       if (!big.empty()) {
         TOMO_TRY(run_subset(big, 2));
         TOMO_TRY(fetch());
-        for (int id : big)
+        for (int id : big) {
           if (flags[id] & (kFlagStray | kFlagBinCap | kFlagOverflow)) safe.push_back(id);
+          else if (flags[id] & kFlagCap) prio.push_back(id);
+        }
+      }
+      if (!prio.empty()) {
+        TOMO_TRY(run_subset(prio, 4));
+        TOMO_TRY(fetch());
+        for (int id : prio)
+          if (flags[id] & kFlagRedo) safe.push_back(id);
       }
     }
     if (!safe.empty()) {
@@ -811,10 +837,9 @@ struct Engine {
     for (int i : *subset) {
       if (flags[i] & kFlagSafeOverflow) return set_error(TOMO_ERR_CAPACITY, "column strip exceeds shared memory");
       if (flags[i] & kFlagGrid) return set_error(TOMO_ERR_CAPACITY, "slot index outside the grid");
-      if (flags[i] & (kFlagStray | kFlagOverflow | kFlagBinCap))
-        return set_error(TOMO_ERR_CAPACITY, "orientation unresolved after the re-runs");
+      if (flags[i] & kFlagRedo) return set_error(TOMO_ERR_CAPACITY, "orientation unresolved after the re-runs");
     }
-    n_safe = n_redo[1] + n_redo[2] + n_redo[3];
+    n_safe = n_redo[1] + n_redo[2] + n_redo[3] + n_redo[4];
     return 0;
   }
 
@@ -868,7 +893,7 @@ struct Engine {
   {
     if (id < 0 || id >= nYPR) return set_error(TOMO_ERR_ARG, "orientation index out of range");
     if (P.n_tri == 0) return set_error(TOMO_ERR_ARG, "empty mesh");
-    if (c < 0 || c > 3) return set_error(TOMO_ERR_ARG, "bad strip configuration");
+    if (c < 0 || c > 4) return set_error(TOMO_ERR_ARG, "bad strip configuration");
     choose_strips(c);
     const int mode = cfg[c].mode;
     const size_t smem = cfg[c].smem;
@@ -883,9 +908,9 @@ struct Engine {
     EngineParams p = base_params(mode);
     p.dump_slot = 0; p.dump_cols = dump_cols.ptr; p.dump_keys = dump_keys.ptr; p.dump_types = dump_types.ptr;
     int cap = 4 * P.n_tri + 4096;
-    TOMO_TRY(reserve_batch(1, mode == 0 ? cap : 1));
-    bind_batch(p, 1, mode == 0 ? cap : INT_MAX, 0, id);
-    if (mode == 0) {
+    TOMO_TRY(reserve_batch(1, mode != 1 ? cap : 1));
+    bind_batch(p, 1, mode != 1 ? cap : INT_MAX, 0, id);
+    if (mode != 1) {
       TOMO_CUDA(launch_batch(p, main, smem, &log));
     } else {
       TOMO_CUDA(launch_bin_count(p, main, &log));
@@ -1062,12 +1087,12 @@ int export_best(Engine& E, int id, std::vector<short>* pix, int* npix, float* vm
   std::vector<unsigned> keys;
   std::vector<short> types;
   int fl = -1;
-  for (int c : {0, 1, 3}) {
+  for (int c : {0, 4, 1, 3}) {
     fl = E.dump_compact(id, c, cols, keys, types);
     if (fl < 0) return fl;
-    if (!(fl & (kFlagStray | kFlagOverflow | kFlagBinCap | kFlagSafeOverflow))) break;
+    if (!(fl & (kFlagRedo | kFlagSafeOverflow))) break;
   }
-  if (fl & (kFlagStray | kFlagOverflow | kFlagBinCap | kFlagSafeOverflow | kFlagGrid))
+  if (fl & (kFlagRedo | kFlagSafeOverflow | kFlagGrid))
     return set_error(TOMO_ERR_CAPACITY, "best orientation could not be exported");
   // occupied columns in slot order: rows[rbeg[j] .. rbeg[j+1]) plus an
   // optional bed row (bed_row[j]); bed-only columns listed separately
@@ -1272,7 +1297,7 @@ int tomoSetOption(int key, int value)
     case TOMO_OPT_FORCE_SAFE: E.force_safe = value ? 1 : 0; return 0;
     case TOMO_OPT_NORMAL_SMEM: if (value < 0 || value > 232448) return TOMO_ERR_ARG; E.normal_smem = value; return 0;
     case TOMO_OPT_EXPORT: E.export_pixels = value ? 1 : 0; return 0;
-    case TOMO_OPT_ADAPTIVE: E.adaptive = value ? 1 : 0; E.adapt_smem = E.adapt_h = 0; return 0;
+    case TOMO_OPT_ADAPTIVE: E.adaptive = value ? 1 : 0; E.adapt_smem = E.adapt_h = E.adapt_cfg = 0; return 0;
     default: return TOMO_ERR_ARG;
   }
 }
@@ -1282,9 +1307,9 @@ int tomoGetStats(long long* out, int n)
   std::lock_guard<std::mutex> lock(g_mutex);
   if (!g_engine || out == nullptr) return TOMO_ERR_ARG;
   const Engine& E = *g_engine;
-  const long long v[8] = {E.G, E.H_sweep, (E.G + std::max(E.H_sweep, 1) - 1) / std::max(E.H_sweep, 1),
-                          E.cfg[0].C, E.n_redo[2], E.nYPR, E.batch, E.n_redo[1] + E.n_redo[3]};
-  for (int i = 0; i < n && i < 8; i++) out[i] = v[i];
+  const long long v[9] = {E.G, E.H_sweep, (E.G + std::max(E.H_sweep, 1) - 1) / std::max(E.H_sweep, 1),
+                          E.cfg[0].C, E.n_redo[2], E.nYPR, E.batch, E.n_redo[1] + E.n_redo[3], E.n_redo[4]};
+  for (int i = 0; i < n && i < 9; i++) out[i] = v[i];
   return 0;
 }
 
@@ -1661,11 +1686,11 @@ extern "C" int tomoSweepStatic(const float* f32info, const int* i32info, const f
     for (int o = 0; o < nb; o++) {
       int fl = g_static_hflags[o];
       if (fl & kFlagGrid) return set_error(TOMO_ERR_CAPACITY, "slot index outside the grid");
-      bool safe = (fl & (kFlagStray | kFlagBinCap)) != 0;
+      bool safe = (fl & (kFlagStray | kFlagBinCap | kFlagCap)) != 0;
       if (!safe && (fl & kFlagOverflow)) {
         fl = static_rerun(X, L, o, 2, st);
         if (fl < 0) return fl;
-        safe = (fl & (kFlagStray | kFlagBinCap | kFlagOverflow)) != 0;
+        safe = (fl & kFlagRedo) != 0;
       }
       if (safe) {
         fl = static_rerun(X, L, o, 1, st);
@@ -1677,8 +1702,7 @@ extern "C" int tomoSweepStatic(const float* f32info, const int* i32info, const f
       }
       if (fl & kFlagSafeOverflow) return set_error(TOMO_ERR_CAPACITY, "column strip exceeds shared memory");
       if (fl & kFlagGrid) return set_error(TOMO_ERR_CAPACITY, "slot index outside the grid");
-      if (fl & (kFlagStray | kFlagOverflow | kFlagBinCap))
-        return set_error(TOMO_ERR_CAPACITY, "orientation unresolved after the re-runs");
+      if (fl & kFlagRedo) return set_error(TOMO_ERR_CAPACITY, "orientation unresolved after the re-runs");
     }
     TOMO_CUDA(cudaMemcpyAsync(g_static_hvof, L.o_vof, sizeof(float) * nb, cudaMemcpyDeviceToHost, st));
     TOMO_CUDA(cudaMemcpyAsync(g_static_hvssf, L.o_vssf, sizeof(float) * nb, cudaMemcpyDeviceToHost, st));
@@ -1916,7 +1940,7 @@ int tomoBatchStats(long long* out, int n)
   if (!g_multi || out == nullptr) return TOMO_ERR_ARG;
   const MultiEngine& M = *g_multi;
   long long orient = 0, redo = 0;
-  for (auto* e : M.meshes) { orient += e->nYPR; redo += e->n_redo[1] + e->n_redo[2] + e->n_redo[3]; }
+  for (auto* e : M.meshes) { orient += e->nYPR; redo += e->n_redo[1] + e->n_redo[2] + e->n_redo[3] + e->n_redo[4]; }
   const long long v[8] = {(long long)M.meshes.size(), orient, (long long)M.graph_nodes, M.graph_kernels,
                           (long long)M.n_tuned, (long long)M.tuned.size(), redo, (long long)(M.last_ms * 1000.0)};
   for (int k = 0; k < n && k < 8; k++) out[k] = v[k];

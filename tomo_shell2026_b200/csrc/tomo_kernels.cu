@@ -281,7 +281,7 @@ __device__ __forceinline__ BinRange bin_range(const EngineParams& p, int o, int 
   load_tri(p, o, t, sh, g, raw);
   BinRange r;
   r.code = 0;
-  if (p.mode == 0) {
+  if (p.mode != 1) {
     const int x0 = max(g.x0, 0), x1 = g.x1;
     if (x1 >= p.G) atomicOr(flag, kFlagGrid);
     r.s0 = min(x0 / p.H, p.S - 1);
@@ -463,7 +463,7 @@ __host__ __device__ inline size_t strip_smem_layout(int mode, int H, int G, int 
   const size_t HG = (size_t)H * G;
   size_t b = round16(sizeof(int) * HG) + round16(sizeof(unsigned) * ((HG + 31) / 32));
   b += round16(sizeof(unsigned) * (size_t)C) + round16(sizeof(short) * (size_t)C);
-  if (mode == 1) b += 2 * round16(sizeof(unsigned) * (size_t)C) + round16((size_t)C);
+  if (mode != 0) b += 2 * round16(sizeof(unsigned) * (size_t)C) + round16((size_t)C);
   const size_t chunk = strip_chunk_bytes();
   const size_t olist = round16(sizeof(short) * HG);
   return b + (chunk > olist ? chunk : olist);
@@ -635,7 +635,7 @@ __device__ ColOut column(const EngineParams& p, const StripSmem& sm, int head, b
         if ((unsigned long long)key < prev && (!found || key > best)) { best = key; found = true; }
       }
       if (!found) break;
-      if (d == kSlotCap) { atomicOr(sflag, kFlagStray); return r; }
+      if (d == kSlotCap) { atomicOr(sflag, kFlagCap); return r; }
       const int t = col_step(s, key_z(best), key_nz(best), p.thr, p.explicit_ss);
       if (dump) dump_key(p, gslot, d, best, t);
       prev = best;
@@ -712,7 +712,7 @@ __device__ __forceinline__ void emit(const EngineParams& p, const StripSmem& sm,
 {
   int bad = 0;
   if (sx < 0 || sx >= p.G || sy < 0 || sy >= p.G) bad = kFlagGrid;
-  else if (sx < xs0 || sx >= xs1) bad = (MODE == 0) ? kFlagStray : -1;
+  else if (sx < xs0 || sx >= xs1) bad = (MODE != 1) ? kFlagStray : -1;
   const unsigned mask = __ballot_sync(__activemask(), bad == 0);
   if (bad) { if (bad > 0) atomicOr(sflag, bad); return; }
   const int lane = threadIdx.x & 31;
@@ -721,10 +721,10 @@ __device__ __forceinline__ void emit(const EngineParams& p, const StripSmem& sm,
   if (lane == leader) base = atomicAdd(nent, __popc(mask));
   base = __shfl_sync(mask, base, leader);
   const int e = base + __popc(mask & ((1u << lane) - 1u));
-  if (e >= p.ent_cap) { atomicOr(sflag, MODE == 0 ? kFlagOverflow : kFlagSafeOverflow); return; }
+  if (e >= p.ent_cap) { atomicOr(sflag, MODE != 1 ? kFlagOverflow : kFlagSafeOverflow); return; }
   const int ls = (sx - xs0) * p.G + sy;
   sm.ekey[e] = make_key(z, nz);
-  if (MODE == 1) { sm.et[e] = t; sm.elo[e] = lo; }
+  if (MODE != 0) { sm.et[e] = t; sm.elo[e] = lo; }
   sm.enext[e] = (short)atomicExch(&sm.heads[ls], e);
 }
 
@@ -777,7 +777,7 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 3 : 1) k_strip(EngineParams p
   sm.ekey = (unsigned*)q; q += round16(sizeof(unsigned) * C);
   sm.enext = (short*)q; q += round16(sizeof(short) * C);
   sm.et = sm.elo = nullptr; sm.emark = nullptr;
-  if (MODE == 1) {
+  if (MODE != 0) {
     sm.et = (unsigned*)q; q += round16(sizeof(unsigned) * C);
     sm.elo = (unsigned*)q; q += round16(sizeof(unsigned) * C);
     sm.emark = (uint8_t*)q; q += round16((size_t)C);
@@ -831,7 +831,7 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 3 : 1) k_strip(EngineParams p
       Bary b;
       bary_setup(g, b);
       int xc0, xc1;
-      if (MODE == 0) { xc0 = max(g.x0, xs0); xc1 = min(g.x1, xs1 - 1); }
+      if (MODE != 1) { xc0 = max(g.x0, xs0); xc1 = min(g.x1, xs1 - 1); }
       else { xc0 = g.x0; xc1 = g.x1; }
       const int ylen = g.y1 - g.y0 + 1;
       if (!fb_only && b.ok && xc0 <= xc1 && ylen > 0) npix = (xc1 - xc0 + 1) * ylen;
@@ -975,7 +975,7 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 3 : 1) k_strip(EngineParams p
     }
   }
   __syncthreads();
-  const bool redo = (MODE == 0) && (sflag & (kFlagStray | kFlagOverflow));
+  const bool redo = (MODE != 1) && (sflag & kFlagRedo);
 
   // ---- phase B: column stage over the occupied slots, contiguous ranges per
   // thread; every occupied column's values go to the slot-ordered fold list
@@ -1020,7 +1020,7 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 3 : 1) k_strip(EngineParams p
     by1 = max(by1, __shfl_xor_sync(0xFFFFFFFFu, by1, off2));
   }
   __syncthreads();
-  const bool redo2 = (MODE == 0) && (sflag & (kFlagStray | kFlagOverflow));
+  const bool redo2 = (MODE != 1) && (sflag & kFlagRedo);
   if (lane == 0 && bx1 >= 0 && !redo2) {
     atomicMin(&p.bbox[o * 4 + 0], bx0); atomicMin(&p.bbox[o * 4 + 1], by0);
     atomicMax(&p.bbox[o * 4 + 2], bx1); atomicMax(&p.bbox[o * 4 + 3], by1);
@@ -1071,7 +1071,7 @@ __global__ void __launch_bounds__(256) k_bed(EngineParams p)
   __shared__ int wsum[8];
   const int o = blockIdx.y;
   const int fl = p.flags[o];
-  if (fl & (kFlagStray | kFlagOverflow | kFlagBinCap)) return;
+  if (fl & kFlagRedo) return;
   const int id = p.ori[o];
   if (p.bed_type == kBedNone || p.bed_r <= 0 || p.bbox[o * 4 + 2] < 0) {
     if (blockIdx.x == 0 && threadIdx.x == 0) p.out_nbed[id] = 0;
@@ -1122,7 +1122,7 @@ __global__ void __launch_bounds__(128) k_fold(EngineParams p)
   const int id = p.ori[o];
   const int fl = p.flags[o];
   if (threadIdx.x == 0) p.out_flags[id] = fl;
-  if (fl & (kFlagStray | kFlagOverflow | kFlagBinCap)) return;
+  if (fl & kFlagRedo) return;
   const long long* a = p.acc + (size_t)o * kAccLanes;
   const int* meta = p.foldmeta + (size_t)o * p.S * 8;
   const long long lim = 1ll << 24;
@@ -1245,9 +1245,9 @@ size_t strip_smem_bytes(int mode, int H, int G, int ent_cap)
 // The strip kernels' dynamic shared-memory limit only ever rises (per
 // device), so every caller's launches stay within it and the attribute is
 // set only when a larger configuration first appears.
-cudaError_t configure_kernels(size_t normal_smem, size_t safe_smem)
+cudaError_t configure_kernels(size_t normal_smem, size_t safe_smem, size_t prio_smem)
 {
-  static size_t conf[64][2];
+  static size_t conf[64][3];
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
@@ -1261,6 +1261,11 @@ cudaError_t configure_kernels(size_t normal_smem, size_t safe_smem)
     e = cudaFuncSetAttribute(k_strip<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)safe_smem);
     if (e != cudaSuccess) return e;
     conf[dev][1] = safe_smem;
+  }
+  if (prio_smem > conf[dev][2]) {
+    e = cudaFuncSetAttribute(k_strip<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)prio_smem);
+    if (e != cudaSuccess) return e;
+    conf[dev][2] = prio_smem;
   }
   return cudaSuccess;
 }
@@ -1318,6 +1323,7 @@ cudaError_t launch_after_count(const EngineParams& p, cudaStream_t main, size_t 
   TOMO_LAUNCH(kKFill, main, (k_bin_fill<<<tri_grid(p), 256, 2 * sizeof(int) * p.S, main>>>(p)));
   const int kind = p.variant == 0 ? kKStrip : kKStripRedo;
   if (p.mode == 0) TOMO_LAUNCH(kind, main, (k_strip<0><<<dim3(p.S, p.Bo), 256, strip_smem, main>>>(p)));
+  else if (p.mode == 2) TOMO_LAUNCH(kind, main, (k_strip<2><<<dim3(p.S, p.Bo), 256, strip_smem, main>>>(p)));
   else TOMO_LAUNCH(kind, main, (k_strip<1><<<dim3(p.S, p.Bo), 256, strip_smem, main>>>(p)));
   TOMO_LAUNCH(kKBed, main, (k_bed<<<dim3(8, p.Bo), 256, 0, main>>>(p)));
   return cudaGetLastError();

@@ -154,10 +154,11 @@ def set_option(key: int, value: int) -> None:
 
 
 def stats() -> dict:
-    out = np.zeros(8, np.int64)
-    lib().tomoGetStats(_p(out, _i64p), 8)
+    out = np.zeros(9, np.int64)
+    lib().tomoGetStats(_p(out, _i64p), 9)
     return dict(grid=int(out[0]), strip_h=int(out[1]), strips=int(out[2]), ent_cap=int(out[3]),
-                overflow_reruns=int(out[4]), n_ypr=int(out[5]), batch=int(out[6]), safe_reruns=int(out[7]))
+                overflow_reruns=int(out[4]), n_ypr=int(out[5]), batch=int(out[6]), safe_reruns=int(out[7]),
+                prio_reruns=int(out[8]))
 
 
 @dataclass
