@@ -341,7 +341,7 @@ def plain_rate(mesh, ypr, opts, n: int = 256) -> dict:
         s.run_device()
         ms = s.run_device()
     finally:
-        native.set_option(native.TOMO_OPT_BATCH, 128)
+        native.set_option(native.TOMO_OPT_BATCH, 256)
     return {"orientations": n, "orientations_per_s": n / (ms / 1000.0), "orientations_per_launch": 1}
 
 
@@ -389,14 +389,16 @@ def _peaks():
 
 
 def _traffic(mesh, res, launches_per_step):
-    """DRAM bytes per k_strip launch from the committed ncu summary, when present."""
+    """DRAM bytes per k_strip launch from the committed ncu summary, when
+    present, scaled from its launch size to this run's orientations per launch."""
     p = ROOT / "profiles" / "k_strip_traffic.json"
-    if not p.exists():
+    if not p.exists() or not launches_per_step:
         return None
     try:
         d = json.loads(p.read_text())
-        return float(d["dram_bytes_per_launch"])
-    except (ValueError, KeyError):
+        per_orientation = float(d["dram_bytes_per_launch"]) / float(d["orientations_per_launch"])
+        return per_orientation * (len(res["Vss64"]) / launches_per_step)
+    except (ValueError, KeyError, ZeroDivisionError):
         return None
 
 

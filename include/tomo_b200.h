@@ -86,7 +86,7 @@ float tomoShadowThreshold(float theta_c);
 void tomoVolToMass(const float* f32info, const int* i32info, float* vm22);
 
 /* Tuning / test hooks. */
-#define TOMO_OPT_BATCH 1        /* orientations per device batch (default 128) */
+#define TOMO_OPT_BATCH 1        /* orientations per device batch (default 256) */
 #define TOMO_OPT_STRIP_H 2      /* force strip height 1, 2, 4 or 8 (0 = automatic) */
 #define TOMO_OPT_FORCE_SAFE 3   /* 1 = evaluate every orientation in safe mode */
 #define TOMO_OPT_NORMAL_SMEM 4  /* shared-memory bytes of a normal strip CTA (0 = 72 KB, three per SM) */

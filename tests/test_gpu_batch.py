@@ -17,7 +17,7 @@ pytestmark = pytest.mark.gpu
 
 
 def _defaults():
-    native.set_option(native.TOMO_OPT_BATCH, 128)
+    native.set_option(native.TOMO_OPT_BATCH, 256)
     native.set_option(native.TOMO_OPT_STRIP_H, 0)
     native.set_option(native.TOMO_OPT_FORCE_SAFE, 0)
     native.set_option(native.TOMO_OPT_NORMAL_SMEM, 0)

@@ -204,7 +204,7 @@ def test_overflow_ladder_and_adaptive_budget(oracle, adaptive):
     finally:
         native.set_option(native.TOMO_OPT_ADAPTIVE, 1)
         native.set_option(native.TOMO_OPT_NORMAL_SMEM, 0)
-        native.set_option(native.TOMO_OPT_BATCH, 128)
+        native.set_option(native.TOMO_OPT_BATCH, 256)
     _compare(res, oracle.sweep(m, ypr, opts), f"adaptive={adaptive}")
     if adaptive:
         assert st["overflow_reruns"] < ypr.shape[0] // 2

@@ -308,7 +308,7 @@ struct Engine {
   // host results of the last sweep
   Params P{};
   int nYPR = 0, G = 0, H = 0, S = 0, ent_cap = 0;
-  int batch = 128;
+  int batch = 256;
   int force_h = 0;        // test hook: strip height override
   int force_safe = 0;     // test hook: run every orientation in safe mode
   int normal_smem = 0;    // shared-memory budget of a normal strip CTA (0 = 72 KB)
