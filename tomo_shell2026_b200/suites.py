@@ -117,6 +117,10 @@ def surrogate_suite(n_meshes: int = 100, seed0: int = 1000, stride: int = 10, ce
     n_yaw, n_pitch = 720, 121
     opts = PrintOptions(explicit_ss=True)
     rows = []
+    # one untimed search first: first-call costs (allocations, kernel loading)
+    warm = meshgen.small_solid(seed0 - 1, with_hull=False)
+    surrogate.search(warm, ypr, n_yaw, n_pitch, opts, stride=stride, cell=cell, top_k=top_k, steps=steps,
+                     margin=margin, holdout=holdout, lr=lr, max_eval=max_eval, log_scale=log_scale)
     for k in range(n_meshes):
         m = meshgen.small_solid(seed0 + k, with_hull=False)
         s = native.Session(m, ypr, opts)
