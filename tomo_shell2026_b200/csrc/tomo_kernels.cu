@@ -155,12 +155,27 @@ __device__ __forceinline__ float centroid(float a, float b, float c)
   return __fadd_rn(__fmul_rn(__fadd_rn(__fadd_rn(a, b), c), 0.333333f), 0.001f);
 }
 
+// Whether any pixel centre of the box passes the barycentric test.  Pixels
+// whose sign-adjusted numerators lie outside the acceptance box by twice the
+// 0.001 margin are rejected before the divisions (the same pre-reject as the
+// strip walk; every such pixel fails the exact test too).
 __device__ bool any_hit(const EngineParams& p, const TriGeo& g, const Bary& b)
 {
   if (!b.ok) return false;
+  const float ad = b.denom >= 0.0f ? b.denom : -b.denom;
+  const bool dpos = b.denom > 0.0f;
+  const float rlo = __fmul_rn(-0.002f, ad), rvhi = __fmul_rn(1.002f, ad), rwhi = __fmul_rn(1.004f, ad);
   for (int x = g.x0; x <= g.x1; x++) {
     const float px = pix_center(x, p.half);
+    const float e2x = __fsub_rn(px, g.ax);
     for (int y = g.y0; y <= g.y1; y++) {
+      const float e2y = __fsub_rn(pix_center(y, p.half), g.ay);
+      const float d20 = dot2(e2x, e2y, b.e0x, b.e0y);
+      const float d21 = dot2(e2x, e2y, b.e1x, b.e1y);
+      const float vn = __fsub_rn(__fmul_rn(b.d11, d20), __fmul_rn(b.d01, d21));
+      const float wn = __fsub_rn(__fmul_rn(b.d00, d21), __fmul_rn(b.d01, d20));
+      const float vs = dpos ? vn : -vn, ws = dpos ? wn : -wn;
+      if (vs < rlo || vs > rvhi || ws < rlo || ws > rwhi) continue;
       float u, v, w;
       if (bary_test(g.ax, g.ay, b, px, pix_center(y, p.half), p.vmax, u, v, w)) return true;
     }
