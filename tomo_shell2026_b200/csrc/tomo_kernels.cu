@@ -463,6 +463,8 @@ struct StripSmem {
   int* pref;           // [kChunk + 4]
   int* thit;           // [kChunk]
   short* olist;        // [H*G] occupied local slots in slot order (aliases the chunk area)
+  unsigned* scr;       // phase B: per-thread key scratch, scr[i * blockDim + thread] (chunk area after olist)
+  int scr_cap;         // keys per thread in scr
 };
 
 __host__ __device__ inline size_t strip_chunk_bytes()
@@ -638,10 +640,39 @@ __device__ ColOut column(const EngineParams& p, const StripSmem& sm, int head, b
     return r;
   }
   int d = 0;
-  if (MODE == 0) {
+  bool need_prio = (MODE == 1);
+  bool sorted = false;
+  unsigned* sc = sm.scr + threadIdx.x;
+  const int st = blockDim.x;
+  int m = 0;
+  if (MODE != 1 && sm.scr_cap > kRegKeys) {
+    // Long list that fits this thread's scratch: copy the keys once, sort
+    // them descending in shared memory, then visit the distinct ones.
+    sorted = true;
+    for (int e = head; e >= 0; e = sm.enext[e]) {
+      if (m == sm.scr_cap) { sorted = false; break; }
+      sc[(m++) * st] = sm.ekey[e];
+    }
+  }
+  if (sorted) {
+    for (int i = 1; i < m; i++) {
+      const unsigned key = sc[i * st];
+      int j = i - 1;
+      while (j >= 0 && sc[j * st] < key) { sc[(j + 1) * st] = sc[j * st]; j--; }
+      sc[(j + 1) * st] = key;
+    }
+    unsigned prev = 0;
+    for (int i = 0; i < m; i++) {
+      const unsigned key = sc[i * st];
+      if (i > 0 && key == prev) continue;
+      if (d == kSlotCap) { need_prio = true; break; }
+      const int t = col_step(s, key_z(key), key_nz(key), p.thr, p.explicit_ss);
+      if (dump) dump_key(p, gslot, d, key, t);
+      prev = key;
+      d++;
+    }
+  } else if (MODE != 1) {
     // Long list, no priorities: visit the distinct keys in descending order.
-    // Past 63 distinct keys the first-come cap decides which survive, which
-    // needs priorities: hand the orientation to safe mode.
     unsigned long long prev = 0x100000000ull;
     for (;;) {
       unsigned best = 0; bool found = false;
@@ -650,13 +681,20 @@ __device__ ColOut column(const EngineParams& p, const StripSmem& sm, int head, b
         if ((unsigned long long)key < prev && (!found || key > best)) { best = key; found = true; }
       }
       if (!found) break;
-      if (d == kSlotCap) { atomicOr(sflag, kFlagCap); return r; }
+      if (d == kSlotCap) { need_prio = true; break; }
       const int t = col_step(s, key_z(best), key_nz(best), p.thr, p.explicit_ss);
       if (dump) dump_key(p, gslot, d, best, t);
       prev = best;
       d++;
     }
-  } else {
+  }
+  // Past 63 distinct keys the first-come cap decides which survive, which
+  // needs priorities: normal strips hand the orientation on; priority strips
+  // start the column over with them.
+  if (need_prio && MODE == 0) { atomicOr(sflag, kFlagCap); return r; }
+  if (need_prio) {
+    col_init(s);
+    d = 0;
     // A pixel is kept iff it is the first (lowest priority) entry of its key
     // and fewer than 63 such first entries precede it (SetBit semantics).
     for (int e = head; e >= 0; e = sm.enext[e]) {
@@ -991,6 +1029,12 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 3 : 1) k_strip(EngineParams p
   }
   __syncthreads();
   const bool redo = (MODE != 1) && (sflag & kFlagRedo);
+  {
+    const size_t ob = round16(sizeof(short) * (size_t)HG);
+    const size_t cb = strip_chunk_bytes();
+    sm.scr = (unsigned*)(chunk + ob);
+    sm.scr_cap = ob < cb ? (int)((cb - ob) / (sizeof(unsigned) * blockDim.x)) : 0;
+  }
 
   // ---- phase B: column stage over the occupied slots, contiguous ranges per
   // thread; every occupied column's values go to the slot-ordered fold list
