@@ -159,6 +159,11 @@ int tomoBatchStats(long long* out, int n);
 /* out4 = orientations per batch, normal-CTA shared-memory budget (0 = 72 KB),
  * strip height, slot-grid edge chosen for mesh `mesh` */
 int tomoBatchConfig(int mesh, int* out4);
+/* The TomoSh_CUDA tail for mesh `mesh` of the last tomoBatchRun: the getters
+ * (getMss, getMo, getVtc, getVolMassInfo, getMat4x4, getnData2i, getpData2i,
+ * getVo64 ...) then return that mesh's results as if TomoSh_CUDA had run on
+ * it alone.  Returns its optID. */
+int tomoBatchExport(int mesh);
 /* key 1: autotune on/off (default 1); key 2: autotune sample orientations (default 512) */
 int tomoBatchSetOption(int key, int value);
 void tomoBatchRelease(void);

@@ -67,3 +67,27 @@ def test_script_runner_on_a_mesh_file(tmp_path):
                                                    bed_type=int(t.BedType[0]), bed_inner=float(t.BedType[1]),
                                                    bed_outer=float(t.BedType[2]), bed_thickness=float(t.BedType[3])))
     assert np.array_equal(r.Mss, t.Mss3D)
+
+
+def test_batched_manager_equals_part_by_part():
+    d = np.load(GOLD)
+    s_o = SlicingOptions()
+    s_o.theta_YP = 30
+    s_o.bVerbose = False
+
+    def group():
+        return CutGroup("pair", [CutObject(f"part{k}", TriMesh(d[f"p{k}_vertices"].astype(np.float64),
+                                                               d[f"p{k}_faces"], d[f"p{k}_vertex_normals"],
+                                                               process=False)) for k in range(2)])
+
+    g1, g2 = group(), group()
+    mgr = TomoManager(s_o)
+    mgr.get_best_orientation(g1)
+    mgr.get_best_orientation_batched(g2)
+    for a, b in zip(g1.cutobjects, g2.cutobjects):
+        ta, tb = a.tomo_object, b.tomo_object
+        assert ta.best_vminfo.vmData == tb.best_vminfo.vmData
+        assert np.array_equal(ta.mat4x4.view(np.int32), tb.mat4x4.view(np.int32))
+        assert [p.type for p in ta.pxl_groups] == [p.type for p in tb.pxl_groups]
+        for pa, pb in zip(ta.pxl_groups, tb.pxl_groups):
+            assert np.array_equal(pa.pxls, pb.pxls)

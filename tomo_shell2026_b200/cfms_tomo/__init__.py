@@ -39,6 +39,14 @@ class TomoManager:
         for c_o in C_G.cutobjects:
             c_o.tomo_object = self.CppDLL.run_dll(c_o, self.slicing_option.bVerbose)
 
+    def get_best_orientation_batched(self, C_G: CutGroup):
+        """get_best_orientation with every part swept in one batched launch
+        (the parts' results are those of get_best_orientation)."""
+        self.name = f"{C_G.name}_tomo"
+        self.input_gr = C_G
+        for c_o, t_o in zip(C_G.cutobjects, self.CppDLL.run_batch(C_G.cutobjects, self.slicing_option.bVerbose)):
+            c_o.tomo_object = t_o
+
     def get_shells(self, offset_size):
         raise NotImplementedError("shell generation belongs to the mesh-cutting package, not this library")
 

@@ -115,6 +115,56 @@ class TomoDLLInterface:
         if self.Cdll_opt_id < 0:
             msg = L.tomoGetLastErrorString()
             raise RuntimeError(f"orientation search failed ({self.Cdll_opt_id}): {msg.decode() if msg else ''}")
+        return self._collect(c_o, T, bVerbose)
+
+    def run_batch(self, cutobjects, bVerbose):
+        """run_dll for every part, all parts swept in one batched graph launch
+        (TomoSh_CUDA_Batch); each part's TomoObject equals run_dll's."""
+        L = self.CppDLL
+        vp = ct.POINTER(ct.c_void_p)
+        L.TomoSh_CUDA_Batch.argtypes = (ct.c_int, vp, vp, vp, vp, vp, vp, ct.POINTER(ct.c_int32))
+        L.TomoSh_CUDA_Batch.restype = ct.c_int32
+        L.tomoBatchExport.argtypes = (ct.c_int,); L.tomoBatchExport.restype = ct.c_int32
+        L.tomoBatchRelease.argtypes = (); L.tomoBatchRelease.restype = None
+        parts, keep = [], []
+        cols = [[] for _ in range(6)]
+        for cutobject0 in cutobjects:
+            if bVerbose:
+                print("Tomo processing: ", cutobject0.name)
+            c_o = deepcopy(cutobject0)
+            self.bShellMesh = self.slicing_option.bShellMesh and (not c_o.tmesh.is_watertight)
+            T = c_o.tmesh
+            vtx = np.asarray(T.vertices).astype(np.float32, copy=True)
+            vtx_nrm = np.asarray(T.vertex_normals).astype(np.float32, copy=True)
+            tri = np.asarray(T.faces).astype(np.int32, copy=True)
+            self.pack(T, self.YPR.shape[0], bVerbose)
+            arrays = (self.Float32Info.copy(), self.Int32Info.copy(), self.YPR, tri, vtx, vtx_nrm)
+            keep.append(arrays)
+            for col, a in zip(cols, arrays):
+                col.append(a.ctypes.data)
+            parts.append((c_o, T))
+        n = len(parts)
+        ptrs = [(ct.c_void_p * max(n, 1))(*c) for c in cols]
+        opt = np.zeros(max(n, 1), np.int32)
+        rc = L.TomoSh_CUDA_Batch(n, *[ct.cast(p, vp) for p in ptrs], opt.ctypes.data_as(ct.POINTER(ct.c_int32)))
+        if rc < 0:
+            msg = L.tomoGetLastErrorString()
+            raise RuntimeError(f"batched orientation search failed ({rc}): {msg.decode() if msg else ''}")
+        out = []
+        try:
+            for k, (c_o, T) in enumerate(parts):
+                self.Cdll_opt_id = L.tomoBatchExport(k)
+                if self.Cdll_opt_id < 0:
+                    msg = L.tomoGetLastErrorString()
+                    raise RuntimeError(f"export of part {k} failed: {msg.decode() if msg else ''}")
+                out.append(self._collect(c_o, T, bVerbose))
+        finally:
+            L.tomoBatchRelease()
+        return out
+
+    def _collect(self, c_o, T, bVerbose):
+        """TomoObject of the last call from the getters (tomo_dll_interface.py:103-133)."""
+        L = self.CppDLL
         t_o = TomoObject(c_o)
 
         Mss3D = np.array(Cptr1d_to_np(L.getMss(), self.YPR.shape[0])).astype(np.float32, copy=True)

@@ -318,6 +318,7 @@ struct Engine {
   int adapt_cfg = 0;                  // 4 once a sweep of this upload switched to priority strips
   float cx = 0, cy = 0, cz = 0;
   std::vector<float> h_rot;
+  std::vector<float> h_vtx;   // the caller's vertices, kept for mat4x4 of a later export
   std::vector<long long> vo64, vss64, vtc64, entries, columns;
   std::vector<float> vof, vssf, vtcf, Mo, Mss, Vtc;
   std::vector<int> nbed, flags;
@@ -453,6 +454,7 @@ struct Engine {
     }
     std::vector<int4> ht(std::max(P.n_tri, 1));
     for (int t = 0; t < P.n_tri; t++) ht[t] = make_int4(tri_h[t * 3 + 0], tri_h[t * 3 + 1], tri_h[t * 3 + 2], 0);
+    h_vtx.assign(vtx, vtx + (size_t)P.n_vtx * 3);
     h_rot.assign((size_t)std::max(nYPR, 1) * 9, 0.f);
     rot_ready.assign((size_t)std::max(nYPR, 1), lazy_rot ? 0 : 1);
     if (lazy_rot) h_ypr.assign(ypr, ypr + (size_t)nYPR * 3);
@@ -1742,6 +1744,7 @@ struct MultiEngine {
   std::vector<Engine::TuneResult> choice;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
+  std::vector<const void*> graph_ptrs;   // every buffer address the captured graph uses
   size_t graph_nodes = 0;
   long long graph_kernels = 0;
   int autotune = 1;
@@ -1753,7 +1756,7 @@ struct MultiEngine {
   {
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
-    exec = nullptr; graph = nullptr; graph_nodes = 0; graph_kernels = 0;
+    exec = nullptr; graph = nullptr; graph_nodes = 0; graph_kernels = 0; graph_ptrs.clear();
   }
   void clear_meshes()
   {
@@ -1812,6 +1815,21 @@ struct MultiEngine {
     return 0;
   }
 
+  std::vector<const void*> buffer_addresses() const
+  {
+    std::vector<const void*> v = {W.xf.ptr, W.minkey.ptr, W.trange.ptr, W.bin_off.ptr, W.bin_cur.ptr, W.bins.ptr,
+                                  W.bbox.ptr, W.bedf.ptr};
+    for (const auto& st : W.set) {
+      v.insert(v.end(), {st.acc.ptr, st.flags.ptr, st.foldcnt.ptr, st.foldv.ptr, st.foldmeta.ptr});
+    }
+    for (const Engine* e : meshes) {
+      v.insert(v.end(), {e->vpos.ptr, e->vnrm.ptr, e->tri.ptr, e->rot.ptr, e->ori.ptr, e->o_vo.ptr, e->o_vss.ptr,
+                         e->o_vtc.ptr, e->o_ent.ptr, e->o_col.ptr, e->o_vof.ptr, e->o_vssf.ptr, e->o_vtcf.ptr,
+                         e->o_nbed.ptr, e->o_flags.ptr});
+    }
+    return v;
+  }
+
   // Every buffer the sweep touches, at its final size, before capture.
   int reserve_all()
   {
@@ -1854,11 +1872,17 @@ struct MultiEngine {
   {
     if (meshes.empty()) return 0;
     TOMO_TRY(reserve_all());
+    // a buffer reallocated since capture (re-runs may grow the bin list)
+    // leaves the graph pointing at freed memory: capture it again
+    if (exec && graph_ptrs != buffer_addresses()) clear_graph();
     cudaEvent_t a = nullptr, b = nullptr;
     TOMO_CUDA(cudaEventCreate(&a));
     TOMO_CUDA(cudaEventCreate(&b));
     int rc = 0;
-    if (use_graph && !exec) rc = capture();
+    if (use_graph && !exec) {
+      rc = capture();
+      graph_ptrs = buffer_addresses();
+    }
     if (rc == 0 && cudaEventRecord(a, W.main) != cudaSuccess) rc = set_error(TOMO_ERR_CUDA, "event record");
     if (rc == 0) {
       if (use_graph) {
@@ -1973,6 +1997,39 @@ int TomoSh_CUDA_Batch(int n_mesh, const float* const* f32info, const int* const*
     if (optIDs) optIDs[m] = o;
   }
   return 0;
+}
+
+// The TomoSh_CUDA tail for mesh `mesh` of the last batch run: its optID's
+// render pixels, vm_info and mat4x4 go to the reference getters (getMss /
+// getMo / getVtc return this mesh's arrays), as if TomoSh_CUDA had just run
+// on it alone.  Returns the optID.
+int tomoBatchExport(int mesh)
+{
+  std::lock_guard<std::mutex> lock(g_mutex);
+  g_last_error = 0; g_last_error_str.clear();
+  if (!g_multi || mesh < 0 || mesh >= (int)g_multi->meshes.size()) return set_error(TOMO_ERR_ARG, "bad mesh index");
+  Engine& E = *g_multi->meshes[mesh];
+  const int n = E.nYPR;
+  if ((int)E.Mss.size() < n) return set_error(TOMO_ERR_ARG, "tomoBatchRun was not called");
+  g_Mss.assign(E.Mss.begin(), E.Mss.begin() + n);
+  g_Mo.assign(E.Mo.begin(), E.Mo.begin() + n);
+  g_Vtc.assign(E.Vtc.begin(), E.Vtc.begin() + n);
+  g_Vo64 = E.vo64; g_Vss64 = E.vss64; g_Vtc64 = E.vtc64;
+  const int opt = first_optimal(n, g_Mss.data());
+  std::memset(g_volmass, 0, sizeof(g_volmass));
+  for (int k = 0; k < 11; k++) { g_pix[k].clear(); g_npix[k] = 0; }
+  if (n > 0) {
+    if (E.P.n_tri > 0) {
+      const int rc = export_best(E, opt, g_pix, g_npix, g_volmass);
+      if (rc) return rc;
+    } else {
+      g_volmass[2] = E.vtcf[opt];
+    }
+    g_volmass[8] = E.vof[opt]; g_volmass[4] = E.vssf[opt];
+    vol_to_mass(E.P, g_volmass);
+    host_mat4x4(E, E.h_vtx.data(), E.P.n_vtx, opt, g_mat4x4);
+  }
+  return opt;
 }
 
 void tomoBatchRelease(void)

@@ -64,6 +64,7 @@ EXPORTS = [
     ("tomoBatchConfig", ct.c_int, [ct.c_int, _i32p]),
     ("tomoBatchSetOption", ct.c_int, [ct.c_int, ct.c_int]),
     ("tomoBatchRelease", None, []),
+    ("tomoBatchExport", ct.c_int, [ct.c_int]),
     ("tomoMlpInit", ct.c_int, [ct.c_int]),
     ("tomoMlpParams", ct.c_int, [_f32p, _f32p]),
     ("tomoMlpGrad", ct.c_int, [_f32p, _f32p, ct.c_int, _f32p, _f32p]),
