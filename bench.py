@@ -297,8 +297,10 @@ def run_ours(args, rank, world, local_rank):
             "traffic": _traffic(mesh, res, strip["launches"] / args.steps),
             "avg_launch_ms": strip_ms / max(strip["timed"], 1),
             "bytes_per_launch": algo_bytes / max(strip["launches"], 1),
-            "kernel_share": {k: (v["ms"] / sum(x["ms"] for x in klog.values())) for k, v in klog.items()
-                             if sum(x["ms"] for x in klog.values()) > 0}}
+            # event spans per kernel kind; the binning kernels (reset .. bin_fill) of batch k+1 run on
+            # their own stream beside batch k's strips, so their spans include time spent waiting for SMs
+            "span_share": {k: (v["ms"] / sum(x["ms"] for x in klog.values())) for k, v in klog.items()
+                           if sum(x["ms"] for x in klog.values()) > 0}}
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,

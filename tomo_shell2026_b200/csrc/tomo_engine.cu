@@ -35,6 +35,8 @@ cudaError_t launch_batch(const EngineParams& p, cudaStream_t main, size_t strip_
 cudaError_t launch_fold(const EngineParams& p, cudaStream_t side, LaunchLog* L);
 cudaError_t launch_bin_count(const EngineParams& p, cudaStream_t main, LaunchLog* L);
 cudaError_t launch_after_count(const EngineParams& p, cudaStream_t main, size_t strip_smem, LaunchLog* L);
+cudaError_t launch_fill(const EngineParams& p, cudaStream_t s, LaunchLog* L);
+cudaError_t launch_strip_bed(const EngineParams& p, cudaStream_t main, size_t strip_smem, LaunchLog* L);
 cudaError_t launch_dump_scan(const int* cols8, int GG, int* off, int* totals, cudaStream_t s);
 cudaError_t launch_zero_ids(int* out, const int* ids, int n, cudaStream_t s);
 cudaError_t launch_gather_outputs(const long long* vo, const long long* vss, const long long* vtc, const long long* ent,
@@ -192,6 +194,20 @@ struct BatchSet {   // per-batch buffers read by the fold, double-buffered
   cudaEvent_t folded = nullptr;
 };
 
+struct PrepSet {    // a batch's rotated vertices and strip bins (binning -> strips)
+  DevBuf<float4> xf;
+  DevBuf<unsigned> minkey;
+  DevBuf<unsigned> trange;
+  DevBuf<int> bin_off, bin_cur, bins, bbox;
+  DevBuf<uint8_t> bedf;
+  cudaEvent_t ready = nullptr;
+  void release()
+  {
+    xf.release(); minkey.release(); trange.release(); bin_off.release(); bin_cur.release(); bins.release();
+    bbox.release(); bedf.release();
+  }
+};
+
 }  // namespace
 
 // ------------------------------------------------ engine
@@ -200,14 +216,10 @@ struct BatchSet {   // per-batch buffers read by the fold, double-buffered
 // (one Workspace per Engine for the single-mesh C-ABI).  Buffers only grow.
 struct Workspace {
   int device = -1;
-  cudaStream_t main = nullptr, side = nullptr;
+  cudaStream_t main = nullptr, side = nullptr, binning = nullptr;
   cudaEvent_t ev_ready = nullptr;
   size_t smem_optin = 0;
-  DevBuf<float4> xf;
-  DevBuf<unsigned> minkey;
-  DevBuf<unsigned> trange;
-  DevBuf<int> bin_off, bin_cur, bins, bbox;
-  DevBuf<uint8_t> bedf;
+  PrepSet prep[2];   // prep[0] is also the single set of the one-batch paths
   BatchSet set[2];
   DevBuf<int> dump_cols;
   DevBuf<unsigned> dump_keys;
@@ -225,8 +237,10 @@ struct Workspace {
     device = dev;
     TOMO_CUDA(cudaStreamCreateWithFlags(&main, cudaStreamNonBlocking));
     TOMO_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+    TOMO_CUDA(cudaStreamCreateWithFlags(&binning, cudaStreamNonBlocking));
     TOMO_CUDA(cudaEventCreateWithFlags(&ev_ready, cudaEventDisableTiming));
     for (auto& s : set) TOMO_CUDA(cudaEventCreateWithFlags(&s.folded, cudaEventDisableTiming));
+    for (auto& q : prep) TOMO_CUDA(cudaEventCreateWithFlags(&q.ready, cudaEventDisableTiming));
     int optin = 0;
     TOMO_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     smem_optin = (size_t)optin;
@@ -235,14 +249,15 @@ struct Workspace {
 
   void release()
   {
-    xf.release(); minkey.release(); trange.release(); bin_off.release(); bin_cur.release(); bins.release();
-    bbox.release(); bedf.release();
+    for (auto& q : prep) q.release();
     for (auto& s : set) { s.acc.release(); s.flags.release(); s.foldcnt.release(); s.foldv.release(); s.foldmeta.release(); }
     dump_cols.release(); dump_keys.release(); dump_types.release();
     dump_off.release(); dump_tot.release(); dump_ccols.release(); dump_ckeys.release(); dump_ctypes.release();
     log.destroy();
     if (main) { cudaStreamDestroy(main); main = nullptr; }
     if (side) { cudaStreamDestroy(side); side = nullptr; }
+    if (binning) { cudaStreamDestroy(binning); binning = nullptr; }
+    for (auto& q : prep) if (q.ready) { cudaEventDestroy(q.ready); q.ready = nullptr; }
     if (ev_ready) { cudaEventDestroy(ev_ready); ev_ready = nullptr; }
     for (auto& s : set) if (s.folded) { cudaEventDestroy(s.folded); s.folded = nullptr; }
   }
@@ -279,8 +294,9 @@ struct Engine {
 
   explicit Engine(Workspace& w, bool owns = false)
       : W(w), owns_ws(owns), device(w.device), main(w.main), side(w.side), ev_ready(w.ev_ready),
-        smem_optin(w.smem_optin), xf(w.xf), minkey(w.minkey), trange(w.trange), bin_off(w.bin_off),
-        bin_cur(w.bin_cur), bins(w.bins), bbox(w.bbox), bedf(w.bedf), set(w.set), dump_cols(w.dump_cols),
+        smem_optin(w.smem_optin), xf(w.prep[0].xf), minkey(w.prep[0].minkey), trange(w.prep[0].trange),
+        bin_off(w.prep[0].bin_off), bin_cur(w.prep[0].bin_cur), bins(w.prep[0].bins), bbox(w.prep[0].bbox),
+        bedf(w.prep[0].bedf), set(w.set), dump_cols(w.dump_cols),
         dump_keys(w.dump_keys), dump_types(w.dump_types), dump_off(w.dump_off), dump_tot(w.dump_tot),
         dump_ccols(w.dump_ccols), dump_ckeys(w.dump_ckeys), dump_ctypes(w.dump_ctypes), log(w.log)
   {
@@ -499,17 +515,20 @@ struct Engine {
     return p;
   }
 
-  int reserve_batch(int Bo, int bin_cap)
+  int reserve_batch(int Bo, int bin_cap, int nprep = 1)
   {
     const size_t GG = (size_t)G * G;
-    TOMO_CUDA(xf.reserve((size_t)Bo * std::max(P.n_vtx, 1)));
-    TOMO_CUDA(minkey.reserve((size_t)Bo * 4));
-    TOMO_CUDA(trange.reserve((size_t)Bo * std::max(P.n_tri, 1)));
-    TOMO_CUDA(bin_off.reserve((size_t)Bo * (S + 1)));
-    TOMO_CUDA(bin_cur.reserve((size_t)Bo * S));
-    TOMO_CUDA(bins.reserve((size_t)Bo * bin_cap));
-    TOMO_CUDA(bbox.reserve((size_t)Bo * 4));
-    TOMO_CUDA(bedf.reserve((size_t)Bo * GG));
+    for (int q = 0; q < nprep; q++) {
+      PrepSet& b = W.prep[q];
+      TOMO_CUDA(b.xf.reserve((size_t)Bo * std::max(P.n_vtx, 1)));
+      TOMO_CUDA(b.minkey.reserve((size_t)Bo * 4));
+      TOMO_CUDA(b.trange.reserve((size_t)Bo * std::max(P.n_tri, 1)));
+      TOMO_CUDA(b.bin_off.reserve((size_t)Bo * (S + 1)));
+      TOMO_CUDA(b.bin_cur.reserve((size_t)Bo * S));
+      TOMO_CUDA(b.bins.reserve((size_t)Bo * bin_cap));
+      TOMO_CUDA(b.bbox.reserve((size_t)Bo * 4));
+      TOMO_CUDA(b.bedf.reserve((size_t)Bo * GG));
+    }
     for (auto& s : set) {
       TOMO_CUDA(s.acc.reserve((size_t)Bo * kAccLanes));
       TOMO_CUDA(s.flags.reserve((size_t)Bo));
@@ -530,13 +549,14 @@ struct Engine {
     return 0;
   }
 
-  void bind_batch(EngineParams& p, int Bo, int bin_cap, int which, int first)
+  void bind_batch(EngineParams& p, int Bo, int bin_cap, int which, int first, int q = 0)
   {
+    const PrepSet& b = W.prep[q];
     p.Bo = Bo;
     p.ori = ori.ptr + first;
-    p.xf = xf.ptr; p.minkey = minkey.ptr; p.trange = trange.ptr;
-    p.bin_off = bin_off.ptr; p.bin_cur = bin_cur.ptr; p.bins = bins.ptr; p.bin_cap = bin_cap;
-    p.bbox = bbox.ptr; p.bedf = bedf.ptr;
+    p.xf = b.xf.ptr; p.minkey = b.minkey.ptr; p.trange = b.trange.ptr;
+    p.bin_off = b.bin_off.ptr; p.bin_cur = b.bin_cur.ptr; p.bins = b.bins.ptr; p.bin_cap = bin_cap;
+    p.bbox = b.bbox.ptr; p.bedf = b.bedf.ptr;
     p.acc = set[which].acc.ptr; p.flags = set[which].flags.ptr;
     p.foldcnt = set[which].foldcnt.ptr; p.foldv = set[which].foldv.ptr; p.foldmeta = set[which].foldmeta.ptr;
   }
@@ -611,18 +631,36 @@ struct Engine {
     const int Bo = std::min(batch, n);
     const int bin_cap = 4 * P.n_tri + 4096;
     TOMO_TRY(reserve_outputs());
-    TOMO_TRY(reserve_batch(Bo, bin_cap));
+    // Two batches in flight: batch k+1's binning (reset, rotate, bin
+    // count / scan / fill) runs on the binning stream into the other
+    // PrepSet while batch k's strips run on main; each batch's fold follows
+    // on the side stream.  A set is rebinned only after the fold of the
+    // batch that last used it.
+    const bool pipe = n > Bo;
+    TOMO_TRY(reserve_batch(Bo, bin_cap, pipe ? 2 : 1));
     if (ids) TOMO_CUDA(launch_zero_ids(o_nbed.ptr, ids, n, main));
     else TOMO_CUDA(cudaMemsetAsync(o_nbed.ptr, 0, sizeof(int) * nYPR, main));
+    if (pipe) {
+      TOMO_CUDA(cudaEventRecord(ev_ready, main));
+      TOMO_CUDA(cudaStreamWaitEvent(W.binning, ev_ready, 0));
+    }
     EngineParams p = base_params(cfg[c].mode);
     int k = 0;
     for (int first = 0; first < n; first += Bo, k++) {
       const int nb = std::min(Bo, n - first);
       const int which = k & 1;
-      if (k >= 2) TOMO_CUDA(cudaStreamWaitEvent(main, set[which].folded, 0));
-      bind_batch(p, nb, bin_cap, which, first);
+      const int q = pipe ? which : 0;
+      cudaStream_t bs = pipe ? W.binning : main;
+      if (k >= 2) TOMO_CUDA(cudaStreamWaitEvent(bs, set[which].folded, 0));
+      bind_batch(p, nb, bin_cap, which, first, q);
       if (ids) p.ori = ids + first;
-      TOMO_CUDA(launch_batch(p, main, cfg[c].smem, &log));
+      TOMO_CUDA(launch_bin_count(p, bs, &log));
+      TOMO_CUDA(launch_fill(p, bs, &log));
+      if (pipe) {
+        TOMO_CUDA(cudaEventRecord(W.prep[q].ready, bs));
+        TOMO_CUDA(cudaStreamWaitEvent(main, W.prep[q].ready, 0));
+      }
+      TOMO_CUDA(launch_strip_bed(p, main, cfg[c].smem, &log));
       TOMO_CUDA(cudaEventRecord(ev_ready, main));
       TOMO_CUDA(cudaStreamWaitEvent(side, ev_ready, 0));
       TOMO_CUDA(launch_fold(p, side, &log));
@@ -1817,8 +1855,10 @@ struct MultiEngine {
 
   std::vector<const void*> buffer_addresses() const
   {
-    std::vector<const void*> v = {W.xf.ptr, W.minkey.ptr, W.trange.ptr, W.bin_off.ptr, W.bin_cur.ptr, W.bins.ptr,
-                                  W.bbox.ptr, W.bedf.ptr};
+    std::vector<const void*> v;
+    for (const auto& q : W.prep)
+      v.insert(v.end(), {q.xf.ptr, q.minkey.ptr, q.trange.ptr, q.bin_off.ptr, q.bin_cur.ptr, q.bins.ptr, q.bbox.ptr,
+                         q.bedf.ptr});
     for (const auto& st : W.set) {
       v.insert(v.end(), {st.acc.ptr, st.flags.ptr, st.foldcnt.ptr, st.foldv.ptr, st.foldmeta.ptr});
     }
@@ -1838,7 +1878,7 @@ struct MultiEngine {
       e->choose_strips(0);
       TOMO_TRY(e->configure());
       TOMO_TRY(e->reserve_outputs());
-      TOMO_TRY(e->reserve_batch(std::min(e->batch, e->nYPR), 4 * e->P.n_tri + 4096));
+      TOMO_TRY(e->reserve_batch(std::min(e->batch, e->nYPR), 4 * e->P.n_tri + 4096, e->nYPR > e->batch ? 2 : 1));
     }
     return 0;
   }

@@ -1376,6 +1376,24 @@ cudaError_t launch_bin_count(const EngineParams& p, cudaStream_t main, LaunchLog
   return cudaGetLastError();
 }
 
+// The binning half of a batch after its count pass (bin fill).
+cudaError_t launch_fill(const EngineParams& p, cudaStream_t s, LaunchLog* L)
+{
+  TOMO_LAUNCH(kKFill, s, (k_bin_fill<<<tri_grid(p), 256, 2 * sizeof(int) * p.S, s>>>(p)));
+  return cudaGetLastError();
+}
+
+// The strip half of a batch (strips, bed).
+cudaError_t launch_strip_bed(const EngineParams& p, cudaStream_t main, size_t strip_smem, LaunchLog* L)
+{
+  const int kind = p.variant == 0 ? kKStrip : kKStripRedo;
+  if (p.mode == 0) TOMO_LAUNCH(kind, main, (k_strip<0><<<dim3(p.S, p.Bo), 256, strip_smem, main>>>(p)));
+  else if (p.mode == 2) TOMO_LAUNCH(kind, main, (k_strip<2><<<dim3(p.S, p.Bo), 256, strip_smem, main>>>(p)));
+  else TOMO_LAUNCH(kind, main, (k_strip<1><<<dim3(p.S, p.Bo), 256, strip_smem, main>>>(p)));
+  TOMO_LAUNCH(kKBed, main, (k_bed<<<dim3(8, p.Bo), 256, 0, main>>>(p)));
+  return cudaGetLastError();
+}
+
 // Remainder of a batch after launch_bin_count (bin fill, strips, bed).
 cudaError_t launch_after_count(const EngineParams& p, cudaStream_t main, size_t strip_smem, LaunchLog* L)
 {
