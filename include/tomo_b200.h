@@ -89,7 +89,7 @@ void tomoVolToMass(const float* f32info, const int* i32info, float* vm22);
 #define TOMO_OPT_BATCH 1        /* orientations per device batch (default 256) */
 #define TOMO_OPT_STRIP_H 2      /* force strip height 1, 2, 4 or 8 (0 = automatic) */
 #define TOMO_OPT_FORCE_SAFE 3   /* 1 = evaluate every orientation in safe mode */
-#define TOMO_OPT_NORMAL_SMEM 4  /* shared-memory bytes of a normal strip CTA (0 = 72 KB, three per SM) */
+#define TOMO_OPT_NORMAL_SMEM 4  /* shared-memory bytes of a normal strip CTA (0 = the largest that keeps four per SM, ~55 KB) */
 #define TOMO_OPT_EXPORT 5       /* 0 = skip the best orientation's pixel export (default 1) */
 #define TOMO_OPT_ADAPTIVE 6     /* 0 = keep the planned strip budget even when early batches overflow (default 1) */
 int tomoSetOption(int key, int value);

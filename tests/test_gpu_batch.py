@@ -60,7 +60,7 @@ def test_batch_matches_single_mesh_calls():
     assert st["graph_nodes"] > 0 and st["graph_kernels"] > 0
     for m in range(len(cases)):
         c = b.config(m)
-        assert c["batch"] in (64, 128, 256) and c["normal_smem"] in (49152, 73728, 101376)
+        assert c["batch"] in (64, 128, 256) and c["normal_smem"] in (0, 73728, 101376)   # 0: four strip CTAs per SM
     native.Batch.release()
 
 

@@ -196,7 +196,7 @@ def test_overflow_ladder_and_adaptive_budget(oracle, adaptive):
     ypr = meshgen.ypr_grid(np.arange(0, 360, 15), np.arange(0, 70, 10))
     opts = PrintOptions()
     native.set_option(native.TOMO_OPT_ADAPTIVE, adaptive)
-    native.set_option(native.TOMO_OPT_NORMAL_SMEM, 24576)
+    native.set_option(native.TOMO_OPT_NORMAL_SMEM, 19456)   # ~100 entries per one-row strip
     native.set_option(native.TOMO_OPT_BATCH, 32)
     try:
         res = native.sweep(m, ypr, opts)

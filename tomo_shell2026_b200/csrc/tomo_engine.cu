@@ -30,6 +30,7 @@
 namespace tomo {
 
 size_t strip_smem_bytes(int mode, int H, int G, int ent_cap);
+size_t strip_four_per_sm_budget();
 cudaError_t configure_kernels(size_t normal_smem, size_t safe_smem, size_t prio_smem);
 cudaError_t launch_batch(const EngineParams& p, cudaStream_t main, size_t strip_smem, LaunchLog* L);
 cudaError_t launch_fold(const EngineParams& p, cudaStream_t side, LaunchLog* L);
@@ -327,7 +328,7 @@ struct Engine {
   int batch = 256;
   int force_h = 0;        // test hook: strip height override
   int force_safe = 0;     // test hook: run every orientation in safe mode
-  int normal_smem = 0;    // shared-memory budget of a normal strip CTA (0 = 72 KB)
+  int normal_smem = 0;    // shared-memory budget of a normal strip CTA (0 = four CTAs per SM)
   int export_pixels = 1;  // rebuild the best orientation's pixels and vm_info (TomoSh_CUDA tail)
   int adaptive = 1;       // raise the entry budget after overflowing early batches (full sweeps)
   int adapt_smem = 0, adapt_h = 0;   // configuration adapted to by an earlier sweep of this upload
@@ -391,7 +392,9 @@ struct Engine {
   void plan_strips()
   {
     const size_t optin = smem_optin ? smem_optin : 232448;
-    const size_t budget0 = std::min<size_t>(optin - 2048, normal_smem ? (size_t)normal_smem : 73728);
+    // default: the largest budget that keeps four CTAs on an SM (~55 KB on B200)
+    const size_t four = strip_four_per_sm_budget();
+    const size_t budget0 = std::min<size_t>(optin - 2048, normal_smem ? (size_t)normal_smem : (four ? four : 73728));
     // the strip kernel also holds ~0.7 KB of static shared memory
     const size_t budget1 = std::min<size_t>(optin, 227 * 1024) - 2048;
     int h0 = 1;
@@ -979,7 +982,7 @@ struct Engine {
   int autotune(int sample, TuneResult* best)
   {
     static const int kBatches[] = {64, 128, 256};
-    static const int kSmem[] = {49152, 73728, 101376};
+    static const int kSmem[] = {0, 73728, 101376};   // 0: four CTAs per SM
     best->batch = batch; best->normal_smem = normal_smem; best->us_per_orientation = 0.0;
     if (nYPR == 0 || P.n_tri == 0) return 0;
     const int n = std::min(nYPR, std::max(sample, 1));

@@ -457,11 +457,10 @@ struct StripSmem {
   unsigned* elo;       // [C] safe mode: pixel index * 2 + twin (priority, minor)
   uint8_t* emark;      // [C] safe mode: first-come marks
   float4* q0; float4* q1; float4* q2;   // [kChunk] margined vertices, vertex-normal z
-  float4* q3;          // [kChunk] centroid fallback position (x, y, z)
   int4* tm;            // [kChunk] t, x0, y0, ylen
-  int2* tm2;           // [kChunk] xc0, kind
   int* pref;           // [kChunk + 4]
-  int* thit;           // [kChunk]
+  unsigned* thit;      // [kChunk / 32] triangles with an accepted pixel
+  uint8_t* tkind;      // [kChunk] bit 0: fallback only; bit 1: box inside one strip
   short* olist;        // [H*G] occupied local slots in slot order (aliases the chunk area)
   unsigned* scr;       // phase B: per-thread key scratch, scr[i * blockDim + thread] (chunk area after olist)
   int scr_cap;         // keys per thread in scr
@@ -469,7 +468,8 @@ struct StripSmem {
 
 __host__ __device__ inline size_t strip_chunk_bytes()
 {
-  return 4 * sizeof(float4) * kChunk + sizeof(int4) * kChunk + sizeof(int2) * kChunk + sizeof(int) * (2 * kChunk + 4);
+  return 3 * sizeof(float4) * kChunk + sizeof(int4) * kChunk + sizeof(int) * (kChunk + 4) + sizeof(unsigned) * (kChunk / 32) +
+         kChunk;
 }
 
 __host__ __device__ inline size_t round16(size_t b) { return (b + 15) / 16 * 16; }
@@ -790,7 +790,9 @@ struct TriReg {
   int t, x0, y0, ylen, xc0;
 };
 
-__device__ __forceinline__ void tri_from_smem(const StripSmem& sm, int ti, TriReg& r)
+// xlo: first slot row of the strip (normal modes) or INT_MIN (safe mode walks
+// the whole box).
+__device__ __forceinline__ void tri_from_smem(const StripSmem& sm, int ti, int xlo, TriReg& r)
 {
   const float4 a4 = sm.q0[ti], b4 = sm.q1[ti], c4 = sm.q2[ti];
   const int4 tm = sm.tm[ti];
@@ -805,11 +807,11 @@ __device__ __forceinline__ void tri_from_smem(const StripSmem& sm, int ti, TriRe
   r.rlo = __fmul_rn(-0.002f, ad);
   r.rvhi = __fmul_rn(1.002f, ad);
   r.rwhi = __fmul_rn(1.004f, ad);
-  r.t = tm.x; r.x0 = tm.y; r.y0 = tm.z; r.ylen = tm.w; r.xc0 = sm.tm2[ti].x;
+  r.t = tm.x; r.x0 = tm.y; r.y0 = tm.z; r.ylen = tm.w; r.xc0 = max(tm.y, xlo);
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(256, MODE == 0 ? 3 : 1) k_strip(EngineParams p)
+__global__ void __launch_bounds__(256, MODE == 0 ? 4 : 1) k_strip(EngineParams p)
 {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ int nent, sflag, wtot[32];
@@ -819,6 +821,7 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 3 : 1) k_strip(EngineParams p
   const int HG = p.H * p.G;
   const int C = p.ent_cap;
   const int xs0 = s * p.H, xs1 = min(xs0 + p.H, p.G);
+  const int xlo = MODE != 1 ? xs0 : INT_MIN;
   const int HGs = (xs1 - xs0) * p.G;   // the last strip may be narrower than H
   const int nwords = (HG + 31) >> 5;
 
@@ -839,11 +842,10 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 3 : 1) k_strip(EngineParams p
   sm.q0 = (float4*)q; q += sizeof(float4) * kChunk;
   sm.q1 = (float4*)q; q += sizeof(float4) * kChunk;
   sm.q2 = (float4*)q; q += sizeof(float4) * kChunk;
-  sm.q3 = (float4*)q; q += sizeof(float4) * kChunk;
   sm.tm = (int4*)q; q += sizeof(int4) * kChunk;
-  sm.tm2 = (int2*)q; q += sizeof(int2) * kChunk;
   sm.pref = (int*)q; q += sizeof(int) * (kChunk + 4);
-  sm.thit = (int*)q; q += sizeof(int) * kChunk;
+  sm.thit = (unsigned*)q; q += sizeof(unsigned) * (kChunk / 32);
+  sm.tkind = (uint8_t*)q; q += kChunk;
   sm.olist = (short*)chunk;
 
   const int* off = p.bin_off + (size_t)o * (p.S + 1);
@@ -879,8 +881,7 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 3 : 1) k_strip(EngineParams p
       const int t = entry & 0x7FFFFFFF;
       const int fb_only = (entry < 0) ? 1 : 0;
       TriGeo g;
-      float4 raw[3];
-      load_tri(p, o, t, sh, g, raw);
+      load_tri(p, o, t, sh, g);
       Bary b;
       bary_setup(g, b);
       int xc0, xc1;
@@ -893,14 +894,10 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 3 : 1) k_strip(EngineParams p
       sm.q0[i] = make_float4(g.ax, g.ay, g.az, g.n0);
       sm.q1[i] = make_float4(g.bx, g.by, g.bz, g.n1);
       sm.q2[i] = make_float4(g.cx, g.cy, g.cz, g.n2);
-      sm.q3[i] = make_float4(centroid(__fsub_rn(raw[0].x, sh.dx), __fsub_rn(raw[1].x, sh.dx), __fsub_rn(raw[2].x, sh.dx)),
-                             centroid(__fsub_rn(raw[0].y, sh.dy), __fsub_rn(raw[1].y, sh.dy), __fsub_rn(raw[2].y, sh.dy)),
-                             centroid(__fsub_rn(raw[0].z, sh.dz), __fsub_rn(raw[1].z, sh.dz), __fsub_rn(raw[2].z, sh.dz)),
-                             0.f);
       sm.tm[i] = make_int4(t, g.x0, g.y0, ylen);
-      sm.tm2[i] = make_int2(xc0, fb_only | (single << 1));
+      sm.tkind[i] = (uint8_t)(fb_only | (single << 1));
     }
-    sm.thit[i] = 0;
+    if (i < kChunk / 32) sm.thit[i] = 0u;
     int total;
     const int start = block_excl_scan(npix, wtot, total);
     sm.pref[i] = start;
@@ -918,7 +915,7 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 3 : 1) k_strip(EngineParams p
       }
       int ti = lo;
       TriReg r;
-      tri_from_smem(sm, ti, r);
+      tri_from_smem(sm, ti, xlo, r);
       const int k = j0 - sm.pref[ti];
       int x = r.xc0 + k / r.ylen;
       int y = r.y0 + k % r.ylen;
@@ -964,12 +961,12 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 3 : 1) k_strip(EngineParams p
         }
         // advance to item j + 1
         if (j + 1 == tnext) {
-          if (hit_any) sm.thit[ti] = 1;
+          if (hit_any) atomicOr(&sm.thit[ti >> 5], 1u << (ti & 31));
           hit_any = false;
           if (j + 1 < j1) {
             ti++;
             while (sm.pref[ti + 1] <= j + 1) ti++;   // skip triangles without pixels here
-            tri_from_smem(sm, ti, r);
+            tri_from_smem(sm, ti, xlo, r);
             x = r.xc0; y = r.y0; yend = r.y0 + r.ylen - 1;
             tnext = sm.pref[ti + 1];
             px = pix_center(x, half);
@@ -983,17 +980,24 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 3 : 1) k_strip(EngineParams p
           ex1 = __fmul_rn(__fsub_rn(px, r.ax), r.b.e1x);
         }
       }
-      if (hit_any) sm.thit[ti] = 1;
+      if (hit_any) atomicOr(&sm.thit[ti >> 5], 1u << (ti & 31));
     }
     __syncthreads();
     // centroid fallback of triangles without any accepted pixel
     if (i < nchunk) {
-      const int kind = sm.tm2[i].y;
-      const bool fb = (kind & 1) || ((kind & 2) && sm.thit[i] == 0);
+      const int kind = sm.tkind[i];
+      const bool fb = (kind & 1) || ((kind & 2) && ((sm.thit[i >> 5] >> (i & 31)) & 1u) == 0u);
       if (fb) {
-        const float4 c3 = sm.q3[i];
         const float n0 = sm.q0[i].w;
         const unsigned t = (unsigned)sm.tm[i].x;
+        // centroid of the translated (unmargined) vertices, reloaded: few triangles take this path
+        const int4 ix = p.tri[t];
+        const float4* X = p.xf + (size_t)o * p.nV;
+        const float4 A = X[ix.x], B = X[ix.y], Cv = X[ix.z];
+        const float3 c3 = make_float3(
+            centroid(__fsub_rn(A.x, sh.dx), __fsub_rn(B.x, sh.dx), __fsub_rn(Cv.x, sh.dx)),
+            centroid(__fsub_rn(A.y, sh.dy), __fsub_rn(B.y, sh.dy), __fsub_rn(Cv.y, sh.dy)),
+            centroid(__fsub_rn(A.z, sh.dz), __fsub_rn(B.z, sh.dz), __fsub_rn(Cv.z, sh.dz)));
         const int sx = __float2int_rz(c3.x), sy = __float2int_rz(c3.y);
         emit<MODE>(p, sm, &nent, &sflag, xs0, xs1, sx, sy, to_i16(c3.z), to_i16(__fmul_rn(n0, 1000.0f)), t, 0u);
         if (p.twin) {
@@ -1295,6 +1299,24 @@ __global__ void __launch_bounds__(256) k_dump_gather(const int* cols8, const uns
 // ---------------------------------------------------------------- launchers
 
 namespace tomo {
+
+// Largest dynamic shared-memory budget that keeps four normal strip CTAs
+// resident per SM (the kernel's registers are bounded for four), or 0.
+size_t strip_four_per_sm_budget()
+{
+  static size_t cache[64];
+  int dev = 0, per_sm = 0, reserved = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 0;
+  if (cache[dev]) return cache[dev];
+  cudaFuncAttributes fa;
+  if (cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev) != cudaSuccess ||
+      cudaFuncGetAttributes(&fa, k_strip<0>) != cudaSuccess)
+    return 0;
+  const long long per_cta = per_sm / 4 / 128 * 128 - reserved - (long long)fa.sharedSizeBytes;
+  cache[dev] = per_cta > 0 ? (size_t)per_cta / 128 * 128 : 0;
+  return cache[dev];
+}
 
 size_t strip_smem_bytes(int mode, int H, int G, int ent_cap)
 {
