@@ -156,7 +156,7 @@ int TomoSh_CUDA_Batch(int n_mesh, const float* const* f32info, const int* const*
  * size classes tuned by the last prepare, size classes tuned so far,
  * orientations re-run, device time of the last run in microseconds */
 int tomoBatchStats(long long* out, int n);
-/* out4 = orientations per batch, normal-CTA shared-memory budget (0 = 72 KB),
+/* out4 = orientations per batch, normal-CTA shared-memory budget (0 = four CTAs per SM),
  * strip height, slot-grid edge chosen for mesh `mesh` */
 int tomoBatchConfig(int mesh, int* out4);
 /* The TomoSh_CUDA tail for mesh `mesh` of the last tomoBatchRun: the getters

@@ -375,7 +375,7 @@ struct Engine {
   }
 
   // Strip configurations.
-  //   0 normal     : H0-column strips, ~72 KB of shared memory (three CTAs
+  //   0 normal     : H0-column strips, ~55 KB of shared memory (four CTAs
   //                  per SM), entries without priorities; H0 is the tallest
   //                  strip with room for two entries per slot;
   //   1 safe       : H0-column strips, whole-box evaluation, priorities,
