@@ -320,6 +320,11 @@ def run_ours(args, rank, world, local_rank):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(mesh, ypr, opts, grid, budget_s=args.cpu_budget_s,
                                             gpu_vss=res["Vss64"])
+        # the same engine on one host thread, on a smaller sample
+        one = cpu_baseline(mesh, ypr, opts, grid, budget_s=args.cpu_budget_s / 2, gpu_vss=res["Vss64"], threads=1)
+        line["cpu_baseline"]["single_thread"] = {k: one[k] for k in ("value", "unit", "cores", "kind", "sample")
+                                                 if k in one}
+        line["cpu_baseline"]["single_thread"]["sample_vss_bit_identical"] = one.get("sample_vss_bit_identical")
     if world == 1 and not args.no_extras:
         line["plain"] = plain_rate(mesh, ypr, opts)
         from tomo_shell2026_b200 import suites
