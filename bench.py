@@ -284,6 +284,15 @@ def run_ours(args, rank, world, local_rank):
     h2d = mesh.n_vtx * 16 * 2 + mesh.n_tri * 16 + n * (9 * 4 + 4)
     d2h = n * (5 * 8 + 5 * 4)
 
+    # ---- L2 read bandwidth from the library's probe (no L2 figure in the measured peaks)
+    l2_gbs = None
+    try:
+        probe = torch.zeros(48 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+        l2_gbs = native.read_bandwidth(probe.data_ptr(), probe.numel() * 4, reps=40)
+        del probe
+    except Exception as exc:   # a measurement aid: never costs the bench line
+        print(f"read probe skipped: {exc}", file=sys.stderr)
+
     # ---- roofline of the dominant kernel (k_strip), live event timing
     peaks = _peaks()
     strip = klog["k_strip"]
@@ -299,6 +308,8 @@ def run_ours(args, rank, world, local_rank):
             "bytes_per_launch": algo_bytes / max(strip["launches"], 1),
             # event spans per kernel kind; the binning kernels (reset .. bin_fill) of batch k+1 run on
             # their own stream beside batch k's strips, so their spans include time spent waiting for SMs
+            "l2_read_gbs": l2_gbs, "frac_of_l2": (achieved / l2_gbs) if (achieved and l2_gbs) else None,
+            "l2_source": "the library's read probe over a 48 MB buffer, 40 passes after one untimed pass",
             "span_share": {k: (v["ms"] / sum(x["ms"] for x in klog.values())) for k, v in klog.items()
                            if sum(x["ms"] for x in klog.values()) > 0}}
 

@@ -121,6 +121,13 @@ int tomoFinish(float* Mo, float* Mss, float* Vtc);
 int tomoProfile(int enable, int reset);
 int tomoGetKernelLog(long long* launches, double* ms, long long* timed, int n);
 
+/* Read-bandwidth probe (no counterpart in the reference; a measurement aid):
+ * one untimed pass, then `reps` timed passes of a kernel that reads the
+ * caller's device buffer (16-byte aligned, `bytes` long) through L2;
+ * *ms_out = device time of the timed passes.  A buffer well inside the
+ * 126 MB L2 gives the L2 read bandwidth; a larger one the HBM read bandwidth. */
+int tomoProbeReadBandwidth(const void* dev_buf, long long bytes, int reps, float* ms_out);
+
 /* Slot grid edge G of the prepared mesh (slot id = x * G + y). */
 int tomoGridSize(void);
 

@@ -91,3 +91,17 @@ def test_rejected_inputs():
     # the library stays usable after every rejection
     r = native.sweep(m, ypr, PrintOptions())
     assert r.Mss.size == 2
+
+
+def test_read_probe():
+    """The library's read-bandwidth probe: a positive figure for an
+    L2-resident device buffer, refusals for host memory and misalignment."""
+    import torch
+    buf = torch.zeros(8 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    gbs = native.read_bandwidth(buf.data_ptr(), buf.numel() * 4, reps=4)
+    assert gbs > 100.0
+    host = np.zeros(1024, np.float32)
+    ms = ct.c_float(0.0)
+    L = native.lib()
+    assert L.tomoProbeReadBandwidth(ct.c_void_p(host.ctypes.data), host.nbytes, 1, ct.byref(ms)) == -1
+    assert L.tomoProbeReadBandwidth(ct.c_void_p(buf.data_ptr() + 4), 1024, 1, ct.byref(ms)) == -1

@@ -40,6 +40,7 @@ cudaError_t launch_fill(const EngineParams& p, cudaStream_t s, LaunchLog* L);
 cudaError_t launch_strip_bed(const EngineParams& p, cudaStream_t main, size_t strip_smem, LaunchLog* L);
 cudaError_t launch_dump_scan(const int* cols8, int GG, int* off, int* totals, cudaStream_t s);
 cudaError_t launch_zero_ids(int* out, const int* ids, int n, cudaStream_t s);
+cudaError_t launch_read_probe(const void* buf, long long bytes, int reps, int blocks, cudaStream_t s);
 cudaError_t launch_gather_outputs(const long long* vo, const long long* vss, const long long* vtc, const long long* ent,
                                   const long long* col, const float* vof, const float* vssf, const float* vtcf,
                                   const int* nbed, const int* flags, const int* ids, int n, long long* stage,
@@ -1436,6 +1437,36 @@ int tomoGetKernelLog(long long* launches, double* ms, long long* timed, int n)
     if (timed) timed[k] = L.timed[k];
   }
   return kKinds;
+}
+
+int tomoProbeReadBandwidth(const void* dev_buf, long long bytes, int reps, float* ms_out)
+{
+  std::lock_guard<std::mutex> lock(g_mutex);
+  if (!dev_buf || bytes < 16 || (reinterpret_cast<uintptr_t>(dev_buf) & 15) != 0 || reps <= 0 || !ms_out)
+    return set_error(TOMO_ERR_ARG, "read probe: need a 16-byte aligned device buffer of at least 16 bytes");
+  cudaPointerAttributes pa;
+  if (cudaPointerGetAttributes(&pa, dev_buf) != cudaSuccess || pa.type != cudaMemoryTypeDevice)
+    return set_error(TOMO_ERR_ARG, "read probe: the buffer is not device memory");
+  int dev = 0, sms = 0;
+  TOMO_CUDA(cudaGetDevice(&dev));
+  TOMO_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  cudaStream_t s = nullptr;
+  cudaEvent_t a = nullptr, b = nullptr;
+  int rc = 0;
+  float ms = 0.f;
+  if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess || cudaEventCreate(&a) != cudaSuccess ||
+      cudaEventCreate(&b) != cudaSuccess)
+    rc = set_error(TOMO_ERR_CUDA, "read probe: stream or event creation failed");
+  // one untimed pass brings the buffer into L2 when it fits
+  else if (launch_read_probe(dev_buf, bytes, 1, 8 * sms, s) != cudaSuccess || cudaEventRecord(a, s) != cudaSuccess ||
+           launch_read_probe(dev_buf, bytes, reps, 8 * sms, s) != cudaSuccess || cudaEventRecord(b, s) != cudaSuccess ||
+           cudaEventSynchronize(b) != cudaSuccess || cudaEventElapsedTime(&ms, a, b) != cudaSuccess)
+    rc = set_error(TOMO_ERR_CUDA, "read probe: launch or timing failed");
+  if (a) cudaEventDestroy(a);
+  if (b) cudaEventDestroy(b);
+  if (s) cudaStreamDestroy(s);
+  if (rc == 0) *ms_out = ms;
+  return rc;
 }
 
 int tomoGridSize(void)

@@ -1495,6 +1495,31 @@ __global__ void k_zero_ids(int* out, const int* ids, int n)
 }
 
 // out[ids[i]] = 0 for i < n (per-orientation counters of a subset sweep).
+// Read-bandwidth probe: every thread sums its grid-stride share of buf
+// (n4 float4 elements), reps times, through L2 (ld.global.cg, no L1).  The
+// sum is stored only if it equals an improbable value, so the loads stay
+// live without a store per thread.
+__global__ void __launch_bounds__(256) k_read_probe(const float4* __restrict__ buf, long long n4, int reps, float* out)
+{
+  float acc = 0.f;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const long long first = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  for (int r = 0; r < reps; r++)
+    for (long long i = first; i < n4; i += stride) {
+      const float4 v = __ldcg(buf + i);
+      acc = __fadd_rn(acc, __fadd_rn(__fadd_rn(v.x, v.y), __fadd_rn(v.z, v.w)));
+    }
+  if (acc == 1.2345678e-30f) out[0] = acc;
+}
+
+cudaError_t launch_read_probe(const void* buf, long long bytes, int reps, int blocks, cudaStream_t s)
+{
+  const long long n4 = bytes / (long long)sizeof(float4);
+  if (n4 <= 0 || reps <= 0 || blocks <= 0) return cudaSuccess;
+  k_read_probe<<<blocks, 256, 0, s>>>((const float4*)buf, n4, reps, (float*)buf);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_zero_ids(int* out, const int* ids, int n, cudaStream_t s)
 {
   if (n <= 0) return cudaSuccess;

@@ -53,6 +53,7 @@ EXPORTS = [
     ("tomoFinish", ct.c_int, [_f32p, _f32p, _f32p]),
     ("tomoGridSize", ct.c_int, []),
     ("tomoProfile", ct.c_int, [ct.c_int, ct.c_int]),
+    ("tomoProbeReadBandwidth", ct.c_int, [ct.c_void_p, ct.c_longlong, ct.c_int, ct.POINTER(ct.c_float)]),
     ("tomoGetKernelLog", ct.c_int, [_i64p, ct.POINTER(ct.c_double), _i64p, ct.c_int]),
     ("tomoColumnDump", ct.c_int, [ct.c_int, ct.c_int, _i32p, _u32p, _i16p]),
     ("tomoSweepStatic", ct.c_int, [_f32p, _i32p, _f32p, _i32p, _f32p, _f32p, _f32p, _f32p, _f32p, ct.c_void_p]),
@@ -147,6 +148,13 @@ def kernel_log() -> dict:
     timed = np.zeros(n, np.int64)
     lib().tomoGetKernelLog(_p(launches, _i64p), ms.ctypes.data_as(ct.POINTER(ct.c_double)), _p(timed, _i64p), n)
     return {k: dict(launches=int(launches[i]), ms=float(ms[i]), timed=int(timed[i])) for i, k in enumerate(KERNEL_KINDS)}
+
+
+def read_bandwidth(dev_ptr: int, nbytes: int, reps: int = 40) -> float:
+    """GB/s of the library's read probe over a device buffer (tomoProbeReadBandwidth)."""
+    ms = ct.c_float(0.0)
+    _check(lib().tomoProbeReadBandwidth(ct.c_void_p(dev_ptr), nbytes, reps, ct.byref(ms)))
+    return nbytes * reps / (ms.value * 1e6) if ms.value > 0 else float("nan")
 
 
 def set_option(key: int, value: int) -> None:
