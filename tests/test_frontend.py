@@ -18,7 +18,9 @@ from tomo_shell2026_b200.cfms_tomo import SlicingOptions, TomoDLLInterface, TriM
 from tomo_shell2026_b200.cfms_tomo import tomo_io
 from tomo_shell2026_b200.cfms_tomo.meshio import OrientedBox
 
-REF = Path("/root/reference/cfms_tomo")
+from oracle.build import REF_ROOT  # noqa: E402  (the reference checkout, where present)
+
+REF = REF_ROOT / "cfms_tomo"
 GOLD = Path(__file__).parent / "golden" / "manager_two_parts.npz"
 
 
@@ -151,7 +153,7 @@ def test_trimesh_properties(small):
 @pytest.mark.parametrize("name,faces,watertight", [("(1)sphere.ply", 39200, True), ("(3)manikin.ply", 13672, False),
                                                    ("Bunny_69k.stl", 69662, False)])
 def test_reference_mesh_files(name, faces, watertight):
-    path = Path("/root/reference/MeshData") / name
+    path = REF_ROOT / "MeshData" / name
     if not path.exists():
         pytest.skip("reference mesh data not present")
     m = load(path)

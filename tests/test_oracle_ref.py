@@ -55,10 +55,9 @@ def test_reference_mesh_files_match_reference(oracle, ref_engine, name, scale):
     real geometry with degenerate and tiny triangles; the glTF body is in
     metres, so unscaled it collapses into a few voxels (centroid fallbacks
     everywhere) and scaled to millimetres it is a 166 mm figure."""
-    from pathlib import Path
-
+    from oracle.build import REF_ROOT
     from tomo_shell2026_b200.cfms_tomo import load
-    path = Path("/root/reference/MeshData") / name
+    path = REF_ROOT / "MeshData" / name
     if not path.exists():
         pytest.skip("reference mesh data not present")
     tm = load(path)
