@@ -223,3 +223,20 @@ def test_dense_mesh_first_come_priorities(oracle):
     st = native.stats()
     _compare(res, oracle.sweep(m, ypr, opts), "dense")
     assert st["prio_reruns"] > 0
+
+
+@pytest.mark.parametrize("explicit_ss", [True, False])
+def test_arbitrary_yaw_pitch_roll(oracle, explicit_ss):
+    """Orientations off the yaw/pitch grid: random angles in radians with a
+    non-zero roll, negative and beyond a full turn, over several batches."""
+    rng = np.random.default_rng(22)
+    m = meshgen.small_solid(22)
+    ypr = rng.uniform(-7.0, 7.0, (300, 3)).astype(np.float32)
+    opts = PrintOptions(explicit_ss=explicit_ss, shell_mesh=True, shell_thickness=0.5, bed_type=2, bed_outer=2.0,
+                        bed_thickness=0.97)
+    native.set_option(native.TOMO_OPT_BATCH, 64)
+    try:
+        res = native.sweep(m, ypr, opts)
+    finally:
+        native.set_option(native.TOMO_OPT_BATCH, 256)
+    _compare(res, oracle.sweep(m, ypr, opts), "yaw/pitch/roll")

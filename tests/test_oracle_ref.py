@@ -72,3 +72,18 @@ def test_reference_mesh_files_match_reference(oracle, ref_engine, name, scale):
     for k in KEYS:
         assert np.array_equal(bits(a[k]), bits(b[k])), k
     assert a["optID"] == b["optID"]
+
+
+def test_arbitrary_yaw_pitch_roll_matches_reference(oracle, ref_engine):
+    """Orientations off the yaw/pitch grid: random angles in radians, roll
+    included, negative and beyond a full turn."""
+    rng = np.random.default_rng(21)
+    m = meshgen.small_solid(21, with_hull=False)
+    ypr = rng.uniform(-7.0, 7.0, (48, 3)).astype(np.float32)
+    opts = PrintOptions(explicit_ss=False, shell_mesh=True, shell_thickness=0.5, bed_type=2, bed_outer=2.0,
+                        bed_thickness=0.97)
+    a = oracle.sweep(m, ypr, opts, threads=4)
+    b = ref_engine.sweep(m, ypr, opts, threads=4)
+    for k in KEYS:
+        assert np.array_equal(bits(a[k]), bits(b[k])), k
+    assert a["optID"] == b["optID"]
