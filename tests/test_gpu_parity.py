@@ -240,3 +240,14 @@ def test_arbitrary_yaw_pitch_roll(oracle, explicit_ss):
     finally:
         native.set_option(native.TOMO_OPT_BATCH, 256)
     _compare(res, oracle.sweep(m, ypr, opts), "yaw/pitch/roll")
+
+
+@pytest.mark.parametrize("dvoxel,theta_deg", [(0.5, 30.0), (1.0, 45.0), (2.0, 75.0)])
+@pytest.mark.parametrize("explicit_ss", [True, False])
+def test_voxel_size_and_critical_angle(oracle, dvoxel, theta_deg, explicit_ss):
+    """Printer parameters off their defaults (voxel size, critical angle)."""
+    m = meshgen.small_solid(23)
+    ypr = meshgen.ypr_grid(np.arange(0, 360, 15), np.arange(0, 190, 15))
+    opts = PrintOptions(dVoxel=dvoxel, theta_c=float(np.deg2rad(theta_deg)), explicit_ss=explicit_ss, bed_type=1,
+                        bed_outer=2.0, bed_thickness=0.97)
+    _compare(native.sweep(m, ypr, opts), oracle.sweep(m, ypr, opts), f"dVoxel {dvoxel}, theta_c {theta_deg}")

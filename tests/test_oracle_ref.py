@@ -87,3 +87,20 @@ def test_arbitrary_yaw_pitch_roll_matches_reference(oracle, ref_engine):
     for k in KEYS:
         assert np.array_equal(bits(a[k]), bits(b[k])), k
     assert a["optID"] == b["optID"]
+
+
+@pytest.mark.parametrize("dvoxel,theta_deg", [(0.5, 30.0), (1.0, 45.0), (2.0, 75.0)])
+@pytest.mark.parametrize("explicit_ss", [True, False])
+def test_voxel_size_and_critical_angle_match_reference(oracle, ref_engine, dvoxel, theta_deg, explicit_ss):
+    """Printer parameters off their defaults: the voxel size moves the pixel
+    centres and scales the mass model, the critical angle sets the shadow
+    threshold."""
+    m = meshgen.small_solid(23, with_hull=False)
+    ypr = meshgen.ypr_grid(np.arange(0, 360, 30), np.arange(0, 190, 30))
+    opts = PrintOptions(dVoxel=dvoxel, theta_c=float(np.deg2rad(theta_deg)), explicit_ss=explicit_ss, bed_type=1,
+                        bed_outer=2.0, bed_thickness=0.97)
+    a = oracle.sweep(m, ypr, opts, threads=4)
+    b = ref_engine.sweep(m, ypr, opts, threads=4)
+    for k in KEYS:
+        assert np.array_equal(bits(a[k]), bits(b[k])), k
+    assert a["optID"] == b["optID"]
