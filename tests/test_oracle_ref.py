@@ -104,3 +104,23 @@ def test_voxel_size_and_critical_angle_match_reference(oracle, ref_engine, dvoxe
     for k in KEYS:
         assert np.array_equal(bits(a[k]), bits(b[k])), k
     assert a["optID"] == b["optID"]
+
+
+@pytest.mark.parametrize("case", [
+    dict(wall_thickness=0.4, Fcore=0.3, Fclad=0.9, Fss=0.1, Css=1.5, PLA_density=0.00124),
+    dict(wall_thickness=1.2, Fcore=0.05, Fclad=1.0, Fss=0.35, Css=0.8, PLA_density=0.001121),
+])
+@pytest.mark.parametrize("shell_thickness", [0.5, 1.7, 3.0])
+def test_mass_model_and_shell_offset_match_reference(oracle, ref_engine, case, shell_thickness):
+    """VolToMass inputs (wall, infill fractions, density) and the shell twin
+    offset off their defaults, with both shadow models."""
+    m = meshgen.small_solid(24, with_hull=False)
+    ypr = meshgen.ypr_grid(np.arange(0, 360, 45), np.arange(0, 190, 45))
+    for explicit_ss in (True, False):
+        opts = PrintOptions(explicit_ss=explicit_ss, shell_mesh=True, shell_thickness=shell_thickness, bed_type=3,
+                            bed_inner=1.0, bed_outer=3.0, bed_thickness=0.97, **case)
+        a = oracle.sweep(m, ypr, opts, threads=4)
+        b = ref_engine.sweep(m, ypr, opts, threads=4)
+        for k in KEYS:
+            assert np.array_equal(bits(a[k]), bits(b[k])), (k, explicit_ss)
+        assert a["optID"] == b["optID"]
