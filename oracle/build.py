@@ -26,7 +26,9 @@ from pathlib import Path
 ORACLE_DIR = Path(__file__).resolve().parent
 BUILD_DIR = ORACLE_DIR / "_build"
 REF_OUT = ORACLE_DIR / "_ref"
-REF_ROOT = Path(os.environ.get("TOMO_REFERENCE_ROOT", "/root/reference"))
+# The reference checkout: TOMO_REFERENCE_ROOT when set, else a directory named
+# "reference" beside this repository's root.
+REF_ROOT = Path(os.environ.get("TOMO_REFERENCE_ROOT", str(ORACLE_DIR.parent.parent / "reference")))
 REF_SRC = REF_ROOT / "cfms_tomo" / "Tomo_Shell_vc_src"
 CUDA_INC = Path(os.environ.get("CUDA_HOME", "/usr/local/cuda")) / "include"
 

@@ -11,7 +11,10 @@ from tomo_shell2026_b200.meshgen import MeshArrays
 from tomo_shell2026_b200.options import PrintOptions
 
 # per-case sweep fixtures (manager_*.npz belong to the front-end tests)
-GOLDEN = sorted(p for p in (Path(__file__).parent / "golden").glob("*.npz") if not p.name.startswith("manager_"))
+GOLDEN_DIR = Path(__file__).parent / "golden"
+# the small per-case fixtures (the front-end's and the full-size sweeps' have their own layouts)
+GOLDEN = sorted(p for p in GOLDEN_DIR.glob("*.npz")
+                if not p.name.startswith(("manager_", "mesh_")) and not p.stem.endswith("_full"))
 
 
 def load_case(path):
