@@ -96,7 +96,10 @@ int tomoSetOption(int key, int value);
 
 /* out[0..8] = grid edge, strip height, strips, entry capacity, orientations re-run
  * with a large strip capacity, nYPR, batch, orientations re-run in safe mode,
- * orientations re-run with first-come priorities (a column past the 63 cap) */
+ * orientations re-run with first-come priorities (a column past the 63 cap) --
+ * of the last TomoSh_CUDA-style sweep, zero before the first; out[9..11] = the
+ * same three re-run counts (large capacity, priorities, safe mode) of the last
+ * tomoSweepStatic call.  Returns TOMO_ERR_ARG only for a null `out`. */
 int tomoGetStats(long long* out, int n);
 
 /* Per-orientation results of the last sweep; any pointer may be null. */
@@ -233,14 +236,20 @@ int tomoSurrogateSearch(const float* f32info, const int* i32info, const float* Y
  *     TOMO_ERR_CAPACITY with the limit in tomoGetLastErrorString();
  *   - the scratch's device address is looked up with cudaGetSymbolAddress the
  *     first time a device is used (with that device current), so make the first
- *     call on each device before any stream capture begins;
+ *     call on each device before any stream capture begins; the address is kept
+ *     for the life of the process, so no cudaDeviceReset (which unloads this
+ *     library's device code) may come between two calls on that device;
  *   - nothing has to start at zero: each batch clears what its kernels
  *     accumulate into (the bed pixel counts by cudaMemsetAsync, the rest in
  *     the first kernel);
  *   - the scratch is shared by every call on a device, so two calls whose
  *     device work overlapped would race on it; the call holds the library's
- *     lock and synchronizes `stream` before it returns, so calls from several
+ *     lock and synchronizes `stream` before it returns -- error returns
+ *     included, once any device work was issued -- so calls from several
  *     host threads run one after another;
+ *   - orientations that a strip cannot resolve alone are re-run in the same
+ *     configurations as TomoSh_CUDA (large capacity, first-come priorities,
+ *     safe mode); tomoGetStats out[9..11] counts them for the last call;
  *   - work is issued on `stream` (a cudaStream_t; null = the legacy default
  *     stream), orientations four at a time. */
 int tomoSweepStatic(const float* f32info, const int* i32info, const float* YPR, const int* tri, const float* vtx,

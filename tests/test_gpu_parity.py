@@ -251,3 +251,22 @@ def test_voxel_size_and_critical_angle(oracle, dvoxel, theta_deg, explicit_ss):
     opts = PrintOptions(dVoxel=dvoxel, theta_c=float(np.deg2rad(theta_deg)), explicit_ss=explicit_ss, bed_type=1,
                         bed_outer=2.0, bed_thickness=0.97)
     _compare(native.sweep(m, ypr, opts), oracle.sweep(m, ypr, opts), f"dVoxel {dvoxel}, theta_c {theta_deg}")
+
+
+@pytest.mark.parametrize("case", [
+    dict(wall_thickness=0.4, Fcore=0.3, Fclad=0.9, Fss=0.1, Css=1.5, PLA_density=0.00124),
+    dict(wall_thickness=1.2, Fcore=0.05, Fclad=1.0, Fss=0.35, Css=0.8, PLA_density=0.001121),
+])
+@pytest.mark.parametrize("shell_thickness", [0.5, 1.7, 3.0])
+def test_mass_model_and_shell_offset(oracle, case, shell_thickness):
+    """The library's own VolToMass restatement at mass-model parameters off
+    their defaults (wall, infill fractions, density) and at three shell twin
+    offsets, with a skirt and both shadow models: Mo / Mss / Vtc bits and
+    optID against the oracle (itself pinned against the reference engine at
+    the same parameters)."""
+    m = meshgen.small_solid(24)
+    ypr = meshgen.ypr_grid(np.arange(0, 360, 45), np.arange(0, 190, 45))
+    for explicit_ss in (True, False):
+        opts = PrintOptions(explicit_ss=explicit_ss, shell_mesh=True, shell_thickness=shell_thickness, bed_type=3,
+                            bed_inner=1.0, bed_outer=3.0, bed_thickness=0.97, **case)
+        _compare(native.sweep(m, ypr, opts), oracle.sweep(m, ypr, opts), f"mass model {case}, explicit {explicit_ss}")

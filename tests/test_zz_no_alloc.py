@@ -8,7 +8,7 @@ from __future__ import annotations
 import numpy as np
 import pytest
 
-from tests.test_golden import GOLDEN, bits, load_case
+from tests.test_golden import GOLDEN, GOLDEN_DIR, bits, load_case
 from tomo_shell2026_b200 import meshgen, native
 from tomo_shell2026_b200.options import PrintOptions
 
@@ -67,3 +67,33 @@ def test_static_rejects_beyond_limits():
     wide = meshgen.mesh_from_arrays(small.vertices * 3.0, small.faces, "wide", with_hull=False)
     with pytest.raises(native.TomoError, match="static limit of 256"):
         native.sweep_static(wide, ypr, PrintOptions())
+
+
+def _static_reruns():
+    st = native.stats()
+    return st["static_overflow_reruns"], st["static_prio_reruns"], st["static_safe_reruns"]
+
+
+def test_static_rerun_ladder_first_come_cap():
+    """Columns past the 63-pixel cap (the stacked-layers mesh): the flagged
+    orientations are re-run with first-come priorities, as TomoSh_CUDA does,
+    and the results still equal TomoSh_CUDA's, twice."""
+    _defaults()
+    d, mesh, opts = load_case(GOLDEN_DIR / "layers_cap63.npz")
+    ref = native.sweep(mesh, d["ypr"], opts)
+    for _ in range(2):
+        _same(ref, native.sweep_static(mesh, d["ypr"], opts))
+        assert _static_reruns()[1] > 0, "no orientation took the priority re-run"
+
+
+def test_static_rerun_ladder_dense_mesh():
+    """A dense 16k-triangle sphere (about one triangle per voxel face): strip
+    lists and silhouette columns force re-runs; results equal TomoSh_CUDA's."""
+    _defaults()
+    mesh = meshgen.perturbed_sphere(16000, 30.0, 7, with_hull=False)
+    ypr = meshgen.ypr_grid(np.arange(0, 360, 45), np.arange(0, 61, 30))
+    opts = PrintOptions()
+    ref = native.sweep(mesh, ypr, opts)
+    for _ in range(2):
+        _same(ref, native.sweep_static(mesh, ypr, opts))
+    assert sum(_static_reruns()) > 0, "the dense mesh re-ran nothing"

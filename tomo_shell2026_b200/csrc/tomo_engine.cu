@@ -187,6 +187,9 @@ struct DevBuf {
 // Largest slot grid edge (columns of the rotated footprint at the voxel pitch).
 constexpr int kMaxGrid = 4096;
 
+// Orientations the last tomoSweepStatic call re-ran, per strip configuration.
+int g_static_reruns[5];
+
 struct BatchSet {   // per-batch buffers read by the fold, double-buffered
   DevBuf<long long> acc;
   DevBuf<int> flags;
@@ -1349,11 +1352,18 @@ int tomoSetOption(int key, int value)
 int tomoGetStats(long long* out, int n)
 {
   std::lock_guard<std::mutex> lock(g_mutex);
-  if (!g_engine || out == nullptr) return TOMO_ERR_ARG;
-  const Engine& E = *g_engine;
-  const long long v[9] = {E.G, E.H_sweep, (E.G + std::max(E.H_sweep, 1) - 1) / std::max(E.H_sweep, 1),
-                          E.cfg[0].C, E.n_redo[2], E.nYPR, E.batch, E.n_redo[1] + E.n_redo[3], E.n_redo[4]};
-  for (int i = 0; i < n && i < 9; i++) out[i] = v[i];
+  if (out == nullptr) return TOMO_ERR_ARG;
+  long long v[12] = {0};
+  if (g_engine) {
+    const Engine& E = *g_engine;
+    const long long e[9] = {E.G, E.H_sweep, (E.G + std::max(E.H_sweep, 1) - 1) / std::max(E.H_sweep, 1),
+                            E.cfg[0].C, E.n_redo[2], E.nYPR, E.batch, E.n_redo[1] + E.n_redo[3], E.n_redo[4]};
+    for (int i = 0; i < 9; i++) v[i] = e[i];
+  }
+  v[9] = g_static_reruns[2];
+  v[10] = g_static_reruns[4];
+  v[11] = g_static_reruns[1] + g_static_reruns[3];
+  for (int i = 0; i < n && i < 12; i++) out[i] = v[i];
   return 0;
 }
 
@@ -1503,8 +1513,11 @@ int tomoFinish(float* Mo, float* Mss, float* Vtc)
 // with every device buffer carved out of one file-scope __device__ array
 // and every host buffer a file-scope array, so that a call allocates no
 // memory on the device or the host.  The kernels, the strip configurations
-// and the re-run ladder are those of Engine::execute; only the buffers and
-// the batch size (kStaticBatch orientations) differ.
+// and the re-run ladder are those of Engine::resolve_ids (overflow ->
+// configuration 2, a column past the 63-pixel cap -> priority strips,
+// configuration 4, stray hits or what is still unresolved -> safe mode,
+// configuration 1, then one-column safe strips, configuration 3); only the
+// buffers and the batch size (kStaticBatch orientations) differ.
 
 namespace tomo {
 
@@ -1631,9 +1644,9 @@ int static_rerun(Engine& X, const StaticLayout& L, int slot, int c, cudaStream_t
   EngineParams p = X.base_params(mode);
   p.variant = c;
   const int normal_cap = 4 * X.P.n_tri + 4096;
-  static_bind(p, L, 1, slot, mode == 0 ? normal_cap : INT_MAX);
+  static_bind(p, L, 1, slot, mode != 1 ? normal_cap : INT_MAX);
   TOMO_CUDA(cudaMemsetAsync(L.o_nbed + slot, 0, sizeof(int), st));
-  if (mode == 0) {
+  if (mode != 1) {
     TOMO_CUDA(launch_batch(p, st, X.cfg[c].smem, nullptr));
   } else {
     TOMO_CUDA(launch_bin_count(p, st, nullptr));
@@ -1651,6 +1664,18 @@ int static_rerun(Engine& X, const StaticLayout& L, int slot, int c, cudaStream_t
   TOMO_CUDA(cudaStreamSynchronize(st));
   return fl;
 }
+
+// Synchronizes the call's stream on every return once device work has been
+// issued, so that no kernel of a failed call is still queued on the shared
+// scratch when the library's lock is released.
+struct StreamDrain {
+  cudaStream_t st;
+  bool armed = false;
+  ~StreamDrain()
+  {
+    if (armed) cudaStreamSynchronize(st);
+  }
+};
 
 }  // namespace
 }  // namespace tomo
@@ -1713,6 +1738,7 @@ extern "C" int tomoSweepStatic(const float* f32info, const int* i32info, const f
     vol_to_mass(P, vm);
     Mo[id] = vm[16]; Mss[id] = vm[13]; Vtc[id] = vm[2];
   };
+  for (int& r : g_static_reruns) r = 0;
   if (P.n_ypr == 0) return 0;
   if (P.n_tri == 0) {
     for (int i = 0; i < P.n_ypr; i++) finish(i, 0.f, 0.f, 0.f, 0);
@@ -1720,6 +1746,7 @@ extern "C" int tomoSweepStatic(const float* f32info, const int* i32info, const f
   }
 
   cudaStream_t st = (cudaStream_t)stream;
+  StreamDrain drain{st};   // declared after the lock: runs before it is released
   void* base = nullptr;
   TOMO_TRY(static_arena(&base));
   const StaticLayout L = static_layout((unsigned char*)base, P.n_vtx, P.n_tri);
@@ -1735,6 +1762,7 @@ extern "C" int tomoSweepStatic(const float* f32info, const int* i32info, const f
     g_static_hnrm[v] = make_float4(vtx_nrm[v * 3 + 0], vtx_nrm[v * 3 + 1], vtx_nrm[v * 3 + 2], 0.f);
   }
   for (int t = 0; t < P.n_tri; t++) g_static_htri[t] = make_int4(tri[t * 3 + 0], tri[t * 3 + 1], tri[t * 3 + 2], 0);
+  drain.armed = true;
   TOMO_CUDA(cudaMemcpyAsync(L.vpos, g_static_hpos, sizeof(float4) * P.n_vtx, cudaMemcpyHostToDevice, st));
   TOMO_CUDA(cudaMemcpyAsync(L.vnrm, g_static_hnrm, sizeof(float4) * P.n_vtx, cudaMemcpyHostToDevice, st));
   TOMO_CUDA(cudaMemcpyAsync(L.tri, g_static_htri, sizeof(int4) * P.n_tri, cudaMemcpyHostToDevice, st));
@@ -1756,22 +1784,31 @@ extern "C" int tomoSweepStatic(const float* f32info, const int* i32info, const f
     TOMO_CUDA(launch_fold(p, st, nullptr));
     TOMO_CUDA(cudaMemcpyAsync(g_static_hflags, L.o_flags, sizeof(int) * nb, cudaMemcpyDeviceToHost, st));
     TOMO_CUDA(cudaStreamSynchronize(st));
-    // the re-run ladder of Engine::execute, per flagged slot
+    // the re-run ladder of Engine::resolve_ids, per flagged slot
     for (int o = 0; o < nb; o++) {
       int fl = g_static_hflags[o];
       if (fl & kFlagGrid) return set_error(TOMO_ERR_CAPACITY, "slot index outside the grid");
-      bool safe = (fl & (kFlagStray | kFlagBinCap | kFlagCap)) != 0;
+      bool safe = (fl & (kFlagStray | kFlagBinCap)) != 0;
       if (!safe && (fl & kFlagOverflow)) {
         fl = static_rerun(X, L, o, 2, st);
         if (fl < 0) return fl;
+        g_static_reruns[2]++;
+        safe = (fl & (kFlagStray | kFlagBinCap | kFlagOverflow)) != 0;
+      }
+      if (!safe && (fl & kFlagCap)) {
+        fl = static_rerun(X, L, o, 4, st);
+        if (fl < 0) return fl;
+        g_static_reruns[4]++;
         safe = (fl & kFlagRedo) != 0;
       }
       if (safe) {
         fl = static_rerun(X, L, o, 1, st);
         if (fl < 0) return fl;
+        g_static_reruns[1]++;
         if (fl & kFlagSafeOverflow) {
           fl = static_rerun(X, L, o, 3, st);
           if (fl < 0) return fl;
+          g_static_reruns[3]++;
         }
       }
       if (fl & kFlagSafeOverflow) return set_error(TOMO_ERR_CAPACITY, "column strip exceeds shared memory");

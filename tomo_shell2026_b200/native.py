@@ -163,11 +163,14 @@ def set_option(key: int, value: int) -> None:
 
 
 def stats() -> dict:
-    out = np.zeros(9, np.int64)
-    lib().tomoGetStats(_p(out, _i64p), 9)
+    """Strip plan and re-run counts of the last sweep (``static_*``: of the
+    last tomoSweepStatic call)."""
+    out = np.zeros(12, np.int64)
+    _check(lib().tomoGetStats(_p(out, _i64p), 12))
     return dict(grid=int(out[0]), strip_h=int(out[1]), strips=int(out[2]), ent_cap=int(out[3]),
                 overflow_reruns=int(out[4]), n_ypr=int(out[5]), batch=int(out[6]), safe_reruns=int(out[7]),
-                prio_reruns=int(out[8]))
+                prio_reruns=int(out[8]), static_overflow_reruns=int(out[9]), static_prio_reruns=int(out[10]),
+                static_safe_reruns=int(out[11]))
 
 
 @dataclass
