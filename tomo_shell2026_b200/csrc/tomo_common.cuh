@@ -102,7 +102,8 @@ struct EngineParams {
   int* bbox;            // [Bo][4] min x, min y, max x, max y of occupied slots
   uint8_t* bedf;        // [Bo][G*G]
   int* foldcnt;         // [Bo][S]
-  int4* foldv;          // [Bo][G*G] (vo, vss, tc, local slot)
+  int2* foldv;          // [Bo][G*G] (vo, vss) of each occupied column, in slot order per strip
+  int* foldtc;          // [Bo][G*G] tc of each occupied column (implicit support only, else null)
   int* foldmeta;        // [Bo][S][8] per strip: sum vo, vss, tc, |vss|, |tc|
 
   // per-orientation outputs (indexed by orientation id)

@@ -194,7 +194,8 @@ struct BatchSet {   // per-batch buffers read by the fold, double-buffered
   DevBuf<long long> acc;
   DevBuf<int> flags;
   DevBuf<int> foldcnt;
-  DevBuf<int4> foldv;
+  DevBuf<int2> foldv;
+  DevBuf<int> foldtc;
   DevBuf<int> foldmeta;
   cudaEvent_t folded = nullptr;
 };
@@ -255,7 +256,7 @@ struct Workspace {
   void release()
   {
     for (auto& q : prep) q.release();
-    for (auto& s : set) { s.acc.release(); s.flags.release(); s.foldcnt.release(); s.foldv.release(); s.foldmeta.release(); }
+    for (auto& s : set) { s.acc.release(); s.flags.release(); s.foldcnt.release(); s.foldv.release(); s.foldtc.release(); s.foldmeta.release(); }
     dump_cols.release(); dump_keys.release(); dump_types.release();
     dump_off.release(); dump_tot.release(); dump_ccols.release(); dump_ckeys.release(); dump_ctypes.release();
     log.destroy();
@@ -541,6 +542,7 @@ struct Engine {
       TOMO_CUDA(s.flags.reserve((size_t)Bo));
       TOMO_CUDA(s.foldcnt.reserve((size_t)Bo * S));
       TOMO_CUDA(s.foldv.reserve((size_t)Bo * GG));
+      if (!P.explicit_ss) TOMO_CUDA(s.foldtc.reserve((size_t)Bo * GG));
       TOMO_CUDA(s.foldmeta.reserve((size_t)Bo * S * 8));
     }
     return 0;
@@ -566,6 +568,7 @@ struct Engine {
     p.bbox = b.bbox.ptr; p.bedf = b.bedf.ptr;
     p.acc = set[which].acc.ptr; p.flags = set[which].flags.ptr;
     p.foldcnt = set[which].foldcnt.ptr; p.foldv = set[which].foldv.ptr; p.foldmeta = set[which].foldmeta.ptr;
+    p.foldtc = p.explicit_ss ? nullptr : set[which].foldtc.ptr;
   }
 
   // All orientations in configuration 0, asynchronously on `main`.  With
@@ -1542,7 +1545,7 @@ constexpr size_t static_bytes(size_t nV, size_t nT)
          static_round(16 * B * nV) + static_round(4 * 4 * B) + static_round(4 * B * nT) +
          static_round(4 * B * (S + 1)) + static_round(4 * B * S) + static_round(4 * B * (4 * nT + 4096)) +
          static_round(4 * 4 * B) + static_round(B * GG) + static_round(8 * B * kAccLanes) + static_round(4 * B) +
-         static_round(4 * B * S) + static_round(16 * B * GG) + static_round(4 * B * S * 8) +
+         static_round(4 * B * S) + static_round(8 * B * GG) + static_round(4 * B * GG) + static_round(4 * B * S * 8) +
          5 * static_round(8 * B) + 3 * static_round(4 * B) + 2 * static_round(4 * B);
 }
 static_assert(static_bytes(kStaticMaxVtx, kStaticMaxTri) <= kStaticArenaBytes,
@@ -1556,7 +1559,8 @@ struct StaticLayout {
   unsigned *minkey, *trange;
   uint8_t* bedf;
   long long *acc, *o_vo, *o_vss, *o_vtc, *o_ent, *o_col;
-  int4* foldv;
+  int2* foldv;
+  int* foldtc;
   float *o_vof, *o_vssf, *o_vtcf;
   long long bins_total;   // entries of the bins region
 };
@@ -1585,7 +1589,8 @@ StaticLayout static_layout(unsigned char* base, int nV, int nT)
   L.acc = (long long*)take(8 * B * kAccLanes);
   L.flags = (int*)take(4 * B);
   L.foldcnt = (int*)take(4 * B * S);
-  L.foldv = (int4*)take(16 * B * GG);
+  L.foldv = (int2*)take(8 * B * GG);
+  L.foldtc = (int*)take(4 * B * GG);
   L.foldmeta = (int*)take(4 * B * S * 8);
   L.o_vo = (long long*)take(8 * B); L.o_vss = (long long*)take(8 * B); L.o_vtc = (long long*)take(8 * B);
   L.o_ent = (long long*)take(8 * B); L.o_col = (long long*)take(8 * B);
@@ -1629,6 +1634,7 @@ void static_bind(EngineParams& p, const StaticLayout& L, int nb, int slot, int b
   p.bin_off = L.bin_off; p.bin_cur = L.bin_cur; p.bins = L.bins; p.bin_cap = bin_cap;
   p.acc = L.acc; p.flags = L.flags; p.bbox = L.bbox; p.bedf = L.bedf;
   p.foldcnt = L.foldcnt; p.foldv = L.foldv; p.foldmeta = L.foldmeta;
+  p.foldtc = p.explicit_ss ? nullptr : L.foldtc;
   p.out_vo = L.o_vo; p.out_vss = L.o_vss; p.out_vtc = L.o_vtc; p.out_vof = L.o_vof; p.out_vssf = L.o_vssf;
   p.out_vtcf = L.o_vtcf; p.out_nbed = L.o_nbed; p.out_flags = L.o_flags; p.out_entries = L.o_ent;
   p.out_columns = L.o_col;
@@ -1931,7 +1937,7 @@ struct MultiEngine {
       v.insert(v.end(), {q.xf.ptr, q.minkey.ptr, q.trange.ptr, q.bin_off.ptr, q.bin_cur.ptr, q.bins.ptr, q.bbox.ptr,
                          q.bedf.ptr});
     for (const auto& st : W.set) {
-      v.insert(v.end(), {st.acc.ptr, st.flags.ptr, st.foldcnt.ptr, st.foldv.ptr, st.foldmeta.ptr});
+      v.insert(v.end(), {st.acc.ptr, st.flags.ptr, st.foldcnt.ptr, st.foldv.ptr, st.foldtc.ptr, st.foldmeta.ptr});
     }
     for (const Engine* e : meshes) {
       v.insert(v.end(), {e->vpos.ptr, e->vnrm.ptr, e->tri.ptr, e->rot.ptr, e->ori.ptr, e->o_vo.ptr, e->o_vss.ptr,

@@ -462,7 +462,8 @@ struct StripSmem {
   unsigned* thit;      // [kChunk / 32] triangles with an accepted pixel
   uint8_t* tkind;      // [kChunk] bit 0: fallback only; bit 1: box inside one strip
   short* olist;        // [H*G] occupied local slots in slot order (aliases the chunk area)
-  unsigned* scr;       // phase B: per-thread key scratch, scr[i * blockDim + thread] (chunk area after olist)
+  short* longq;        // [H*G] phase B: positions in olist of columns with three or more raw entries
+  unsigned* scr;       // phase B: per-thread key scratch, scr[i * blockDim + thread] (chunk area after longq)
   int scr_cap;         // keys per thread in scr
 };
 
@@ -482,7 +483,7 @@ __host__ __device__ inline size_t strip_smem_layout(int mode, int H, int G, int 
   b += round16(sizeof(unsigned) * (size_t)C) + round16(sizeof(short) * (size_t)C);
   if (mode != 0) b += 2 * round16(sizeof(unsigned) * (size_t)C) + round16((size_t)C);
   const size_t chunk = strip_chunk_bytes();
-  const size_t olist = round16(sizeof(short) * HG);
+  const size_t olist = 2 * round16(sizeof(short) * HG);   // occupied-slot list + long-column queue
   return b + (chunk > olist ? chunk : olist);
 }
 
@@ -568,6 +569,35 @@ __device__ __forceinline__ void col_result(const EngineParams& p, ColState& s, i
   r.vss = p.explicit_ss ? (s.ssb - s.ssa) : (-s.al + s.be + s.tc - s.nvb + s.nva);
   r.tc = s.tc;
   r.lastz = s.lastz; r.lasttype = s.lasttype; r.has10 = s.has10;
+}
+
+// Column stage of a slot whose list holds one or two raw entries (no sort,
+// no cap, no priorities).  Returns false, touching nothing, for longer lists.
+__device__ __forceinline__ bool column_short(const EngineParams& p, const StripSmem& sm, int head, bool dump,
+                                             int gslot, ColOut& r)
+{
+  const unsigned k0 = sm.ekey[head];
+  const int e1 = sm.enext[head];
+  unsigned k1 = k0;
+  if (e1 >= 0) {
+    if (sm.enext[e1] >= 0) return false;
+    k1 = sm.ekey[e1];
+  }
+  r.vo = r.vss = r.tc = 0;
+  if (k1 == k0) {   // a single distinct pixel: no pairing
+    r.ndist = 1; r.nfin = 1; r.lastz = key_z(k0); r.lasttype = 0;
+    r.has10 = (key_z(k0) == 1 && key_nz(k0) == 0);
+    if (dump) dump_key(p, gslot, 0, k0, 0);
+    return true;
+  }
+  ColState s;
+  col_init(s);
+  const unsigned hi = (k0 > k1) ? k0 : k1, lo = (k0 > k1) ? k1 : k0;
+  const int t0 = col_step(s, key_z(hi), key_nz(hi), p.thr, p.explicit_ss);
+  const int t1 = col_step(s, key_z(lo), key_nz(lo), p.thr, p.explicit_ss);
+  if (dump) { dump_key(p, gslot, 0, hi, t0); dump_key(p, gslot, 1, lo, t1); }
+  col_result(p, s, 2, r);
+  return true;
 }
 
 // Column stage of one slot from its shared-memory list.
@@ -814,7 +844,7 @@ template <int MODE>
 __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 1) k_strip(EngineParams p)
 {
   extern __shared__ __align__(16) unsigned char smem[];
-  __shared__ int nent, sflag, wtot[32];
+  __shared__ int nent, sflag, nlong, wtot[32];
   __shared__ long long red[8][8];
 
   const int s = blockIdx.x, o = blockIdx.y;
@@ -1036,40 +1066,71 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 1) k_strip(EngineParams p
   {
     const size_t ob = round16(sizeof(short) * (size_t)HG);
     const size_t cb = strip_chunk_bytes();
-    sm.scr = (unsigned*)(chunk + ob);
-    sm.scr_cap = ob < cb ? (int)((cb - ob) / (sizeof(unsigned) * blockDim.x)) : 0;
+    sm.longq = (short*)(chunk + ob);
+    sm.scr = (unsigned*)(chunk + 2 * ob);
+    sm.scr_cap = 2 * ob < cb ? (int)((cb - 2 * ob) / (sizeof(unsigned) * blockDim.x)) : 0;
   }
 
-  // ---- phase B: column stage over the occupied slots, contiguous ranges per
-  // thread; every occupied column's values go to the slot-ordered fold list
-  const int per = (nocc + blockDim.x - 1) / blockDim.x;
-  const int l0 = min((int)threadIdx.x * per, nocc), l1 = min(l0 + per, nocc);
-  long long a_vo = 0, a_vss = 0, a_tc = 0, a_avss = 0, a_atc = 0, a_ent = 0;
+  // ---- phase B: column stage over the occupied slots; every occupied
+  // column's values go to the slot-ordered fold list.  B1 walks the occupied
+  // list lane by lane (a warp takes 32 consecutive columns) and resolves the
+  // columns of one or two raw entries -- almost all of them -- on the spot;
+  // longer columns are queued and B2 takes them one per thread, so that the
+  // few long lists do not hold up the lanes of the short ones.
+  long long a_vo = 0, a_vss = 0, a_tc = 0, a_avss = 0, a_atc = 0, a_ent = 0, a_col = 0;
   int bx0 = INT_MAX, by0 = INT_MAX, bx1 = -1, by1 = -1;
   const bool dump = (o == p.dump_slot) && p.dump_cols != nullptr;
-  int4* fv = p.foldv + (size_t)o * p.G * p.G + (size_t)xs0 * p.G;
+  int2* fv = p.foldv + (size_t)o * p.G * p.G + (size_t)xs0 * p.G;
+  int* ftc = p.foldtc ? p.foldtc + (size_t)o * p.G * p.G + (size_t)xs0 * p.G : nullptr;
+  auto store = [&](int l, int ls, int gx, int gy, int gslot, const ColOut& c) {
+    fv[l] = make_int2(c.vo, c.vss);
+    if (ftc) ftc[l] = c.tc;   // tc is zero with explicit support
+    a_vo += c.vo; a_vss += c.vss; a_tc += c.tc;
+    a_avss += (c.vss < 0) ? -c.vss : c.vss; a_atc += (c.tc < 0) ? -c.tc : c.tc;
+    a_ent += c.ndist;
+    a_col++;
+    bx0 = min(bx0, gx); bx1 = max(bx1, gx); by0 = min(by0, gy); by1 = max(by1, gy);
+    if (p.bed_type != kBedNone) bedf[ls] = bed_flags(p, c);
+    if (dump) {
+      int* d = p.dump_cols + (size_t)gslot * 8;
+      d[0] = c.ndist; d[1] = c.nfin; d[2] = c.vo; d[3] = c.vss; d[4] = c.tc; d[5] = c.lastz;
+      d[6] = c.lasttype; d[7] = (p.bed_type != kBedNone) ? bed_flags(p, c) : 0;
+    }
+  };
+  if (threadIdx.x == 0) nlong = 0;
+  __syncthreads();
   if (!redo) {
-    for (int l = l0; l < l1; l++) {
+    for (int l = threadIdx.x; l < nocc; l += blockDim.x) {
+      const int ls = sm.olist[l];
+      const int gx = xs0 + ls / p.G, gy = ls % p.G;
+      const int gslot = gx * p.G + gy;
+      ColOut c;
+      const bool ok = column_short(p, sm, sm.heads[ls], dump, gslot, c);
+      if (ok) store(l, ls, gx, gy, gslot, c);
+      const unsigned want = __ballot_sync(__activemask(), !ok);
+      if (!ok) {
+        const int lane = threadIdx.x & 31, leader = __ffs(want) - 1;
+        int base = 0;
+        if (lane == leader) base = atomicAdd(&nlong, __popc(want));
+        base = __shfl_sync(want, base, leader);
+        sm.longq[base + __popc(want & ((1u << lane) - 1u))] = (short)l;
+      }
+    }
+  }
+  __syncthreads();
+  if (!redo) {
+    for (int q = threadIdx.x; q < nlong; q += blockDim.x) {
+      const int l = sm.longq[q];
       const int ls = sm.olist[l];
       const int gx = xs0 + ls / p.G, gy = ls % p.G;
       const int gslot = gx * p.G + gy;
       const ColOut c = column<MODE>(p, sm, sm.heads[ls], dump, gslot, &sflag);
-      fv[l] = make_int4(c.vo, c.vss, c.tc, ls);
-      a_vo += c.vo; a_vss += c.vss; a_tc += c.tc;
-      a_avss += (c.vss < 0) ? -c.vss : c.vss; a_atc += (c.tc < 0) ? -c.tc : c.tc;
-      a_ent += c.ndist;
-      bx0 = min(bx0, gx); bx1 = max(bx1, gx); by0 = min(by0, gy); by1 = max(by1, gy);
-      if (p.bed_type != kBedNone) bedf[ls] = bed_flags(p, c);
-      if (dump) {
-        int* d = p.dump_cols + (size_t)gslot * 8;
-        d[0] = c.ndist; d[1] = c.nfin; d[2] = c.vo; d[3] = c.vss; d[4] = c.tc; d[5] = c.lastz;
-        d[6] = c.lasttype; d[7] = (p.bed_type != kBedNone) ? bed_flags(p, c) : 0;
-      }
+      store(l, ls, gx, gy, gslot, c);
     }
   }
 
   // ---- phase C: reductions
-  long long vals[8] = {a_vo, a_vss, a_tc, a_avss, a_atc, a_ent, (long long)(l1 - l0), 0};
+  long long vals[8] = {a_vo, a_vss, a_tc, a_avss, a_atc, a_ent, a_col, 0};
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
   for (int k = 0; k < 7; k++) {
@@ -1177,7 +1238,8 @@ constexpr int kFoldChunk = 1024;
 
 __global__ void __launch_bounds__(128) k_fold(EngineParams p)
 {
-  __shared__ int4 stage[kFoldChunk];
+  __shared__ int2 stage[kFoldChunk];
+  __shared__ int stage_tc[kFoldChunk];
   __shared__ int s_start;
   __shared__ float s_f[3];
   const int o = blockIdx.x;
@@ -1214,18 +1276,22 @@ __global__ void __launch_bounds__(128) k_fold(EngineParams p)
   float fo = s_f[0], fs = s_f[1], ft = s_f[2];
   for (int s = start; s < p.S; s++) {
     const int n = p.foldcnt[(size_t)o * p.S + s];
-    const int4* v = p.foldv + (size_t)o * p.G * p.G + (size_t)s * p.H * p.G;
+    const int2* v = p.foldv + (size_t)o * p.G * p.G + (size_t)s * p.H * p.G;
+    const int* vt = p.foldtc ? p.foldtc + (size_t)o * p.G * p.G + (size_t)s * p.H * p.G : nullptr;
     for (int c0 = 0; c0 < n; c0 += kFoldChunk) {
       const int m = min(kFoldChunk, n - c0);
       __syncthreads();
-      for (int k = threadIdx.x; k < m; k += blockDim.x) stage[k] = v[c0 + k];
+      for (int k = threadIdx.x; k < m; k += blockDim.x) {
+        stage[k] = v[c0 + k];
+        stage_tc[k] = vt ? vt[c0 + k] : 0;
+      }
       __syncthreads();
       if (threadIdx.x == 0) {
         for (int k = 0; k < m; k++) {
-          const int4 x = stage[k];
+          const int2 x = stage[k];
           fo = __fadd_rn(fo, (float)x.x);
           fs = __fadd_rn(fs, (float)x.y);
-          ft = __fadd_rn(ft, (float)x.z);
+          ft = __fadd_rn(ft, (float)stage_tc[k]);
         }
       }
     }
