@@ -17,8 +17,9 @@ C-ABI call TomoSh_CUDA with host buffers; ``roofline`` rates the dominant
 kernel (k_strip) against the measured HBM copy bandwidth; ``cpu_baseline``
 is the reference INT3 engine (built from the reference sources) on the
 host cores over a bounded sample of the same orientations.  With N > 1
-(torchrun) every rank sweeps its own seeded mesh: weak scaling, no
-collective on the data path.
+(torchrun) the ranks split the one headline sweep into contiguous
+orientation shards (strong scaling: the total work is the same at every N)
+and combine the optimum with one MIN all-reduce; nothing else crosses ranks.
 """
 from __future__ import annotations
 
@@ -226,8 +227,11 @@ def run_ours(args, rank, world, local_rank):
     dist = None
     if world > 1:
         import torch.distributed as dist
-    mesh, ypr, opts = workload(rank, args.max_orientations)
-    n = ypr.shape[0]
+    from tomo_shell2026_b200 import sharding
+    mesh, ypr_all, opts = workload(0, args.max_orientations)
+    n = ypr_all.shape[0]
+    b, e = sharding.shard_range(n, rank, world)
+    ypr = np.ascontiguousarray(ypr_all[b:e])
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
     sess = native.Session(mesh, ypr, opts)
@@ -253,36 +257,40 @@ def run_ours(args, rank, world, local_rank):
         dist.barrier()
     klog = native.kernel_log()
     native.profile(False, reset=False)
-    res = native.results(n)
+    res = native.results(e - b)
     opt, Mo, Mss, Vtc = sess.finish()
+    if dist:
+        opt = sharding.global_first_optimal(Mss, b, n)
     total_ms = float(sum(step_ms))
     if dist:
         t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_ms = float(t.item())
-    value = world * args.steps * n / (total_ms / 1000.0)
+    value = args.steps * n / (total_ms / 1000.0)
 
-    # ---- e2e: reference C-ABI with host buffers (H2D + D2H inside)
+    # ---- e2e: reference C-ABI with host buffers (H2D + D2H inside); with
+    # N > 1 each rank's TomoSh_CUDA call sweeps its shard and the optimum is
+    # combined across ranks inside the timed region
     for _ in range(args.warmup):
-        native.sweep(mesh, ypr, opts)
+        sharding.sweep_shard(mesh, ypr_all, opts)
     e2e_s = []
     for _ in range(max(1, args.steps)):
         if dist:
             dist.barrier()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        r = native.sweep(mesh, ypr, opts)
+        r = sharding.sweep_shard(mesh, ypr_all, opts)
         torch.cuda.synchronize()
         e2e_s.append(time.perf_counter() - t0)
-        assert r.optID == opt and np.array_equal(r.Vss64, res["Vss64"]), "e2e run differs from the device run"
+        assert r.optID == opt and np.array_equal(r.shard.Vss64, res["Vss64"]), "e2e run differs from the device run"
     e2e_total = float(sum(e2e_s))
     if dist:
         t = torch.tensor([e2e_total], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_total = float(t.item())
-    e2e_value = world * len(e2e_s) * n / e2e_total
-    h2d = mesh.n_vtx * 16 * 2 + mesh.n_tri * 16 + n * (9 * 4 + 4)
-    d2h = n * (5 * 8 + 5 * 4)
+    e2e_value = len(e2e_s) * n / e2e_total
+    h2d = mesh.n_vtx * 16 * 2 + mesh.n_tri * 16 + (e - b) * (9 * 4 + 4)
+    d2h = (e - b) * (5 * 8 + 5 * 4)
 
     # ---- L2 read bandwidth from the library's probe (no L2 figure in the measured peaks)
     l2_gbs = None
@@ -306,17 +314,18 @@ def run_ours(args, rank, world, local_rank):
             "traffic": _traffic(mesh, res, strip["launches"] / args.steps),
             "avg_launch_ms": strip_ms / max(strip["timed"], 1),
             "bytes_per_launch": algo_bytes / max(strip["launches"], 1),
-            # event spans per kernel kind; the binning kernels (reset .. bin_fill) of batch k+1 run on
-            # their own stream beside batch k's strips, so their spans include time spent waiting for SMs
             "l2_read_gbs": l2_gbs, "frac_of_l2": (achieved / l2_gbs) if (achieved and l2_gbs) else None,
             "l2_source": "the library's read probe over a 48 MB buffer, 40 passes after one untimed pass",
-            "span_share": {k: (v["ms"] / sum(x["ms"] for x in klog.values())) for k, v in klog.items()
-                           if sum(x["ms"] for x in klog.values()) > 0}}
+            # Event spans per kernel kind and step, each on its launching stream.  These are stream spans,
+            # not kernel times: the binning kernels of batch k+1 run on their own stream beside batch k's
+            # strips, so their spans include time spent waiting for SMs and for the other stream.  The
+            # per-kernel breakdown is the serialised ncu launch list summarised under profiles/.
+            "stream_spans_ms_per_step": {k: v["ms"] / args.steps for k, v in klog.items() if v["timed"]}}
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-            "config": config(mesh, ypr, grid, {"parallelism": f"orientation sweep per GPU x{world}",
+            "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+            "config": config(mesh, ypr_all, grid, {"parallelism": f"orientation shards x{world}",
                                                 "batch_orientations": native.stats()["batch"],
                                                 "strip_h": native.stats()["strip_h"]}),
             "time_to_exact_optimum_s": total_ms / args.steps / 1000.0,
