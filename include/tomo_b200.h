@@ -152,7 +152,8 @@ int tomoColumnDump(int ypr_index, int safe_mode, int* cols8, unsigned* keys64, s
  * (autotuner); tomoBatchRun sweeps all meshes -- with use_graph, as one CUDA
  * graph captured on the first run and replayed after -- re-runs flagged
  * orientations per mesh and leaves per-mesh results equal to TomoSh_CUDA on
- * that mesh alone; device_ms receives the device time of the sweep.
+ * that mesh alone; device_ms receives the time on the library's stream from
+ * the start of the sweep until every mesh is resolved (re-runs included).
  * tomoBatchResults copies mesh `mesh`'s per-orientation results (any pointer
  * may be null) and returns its optID.  TomoSh_CUDA_Batch = prepare + run with
  * the graph + optIDs[n_mesh]. */
@@ -164,7 +165,8 @@ int TomoSh_CUDA_Batch(int n_mesh, const float* const* f32info, const int* const*
                       const int* const* tri, const float* const* vtx, const float* const* vtx_nrm, int* optIDs);
 /* out[0..7] = meshes, orientations, graph nodes, kernels per graph launch,
  * size classes tuned by the last prepare, size classes tuned so far,
- * orientations re-run, device time of the last run in microseconds */
+ * orientations re-run, time of the last run in microseconds (sweep and
+ * re-runs, as device_ms), time of its sweep alone (the graph replay) */
 int tomoBatchStats(long long* out, int n);
 /* out4 = orientations per batch, normal-CTA shared-memory budget (0 = four CTAs per SM),
  * strip height, slot-grid edge chosen for mesh `mesh` */

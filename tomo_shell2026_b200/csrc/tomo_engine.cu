@@ -338,6 +338,7 @@ struct Engine {
   int adaptive = 1;       // raise the entry budget after overflowing early batches (full sweeps)
   int adapt_smem = 0, adapt_h = 0;   // configuration adapted to by an earlier sweep of this upload
   int adapt_cfg = 0;                  // 4 once a sweep of this upload switched to priority strips
+  int start_cfg = 0;                  // 4: every sweep starts in priority strips (set by the batch autotuner)
   float cx = 0, cy = 0, cz = 0;
   std::vector<float> h_rot;
   std::vector<float> h_vtx;   // the caller's vertices, kept for mat4x4 of a later export
@@ -634,7 +635,7 @@ struct Engine {
 
   int sweep_batches(const int* ids, int n, bool adapt)
   {
-    int c = (adapt && adapt_cfg == 4) ? 4 : 0;
+    int c = (start_cfg == 4 || (adapt && adapt_cfg == 4)) ? 4 : 0;
     choose_strips(c);
     H_sweep = H;
     TOMO_TRY(configure());
@@ -985,12 +986,25 @@ struct Engine {
   // height, the entry capacity and the CTAs per SM) and keeps the fastest.
   // Only the speed depends on the choice: every configuration's results are
   // exact (overflowing strips are re-run).
-  struct TuneResult { int batch, normal_smem; double us_per_orientation; };
+  // Strip configuration of a sweep picked by the batch autotuner.
+  struct TuneResult { int batch, normal_smem, strip_h, start_cfg; double us_per_orientation; };
+
+  // Times candidate configurations on an evenly strided sample of the
+  // orientations and keeps the fastest.  A candidate's time covers the whole
+  // sweep of the sample, re-runs included: the configuration-0 strips, then
+  // the ladder that re-runs what they flagged (Engine::resolve), so a budget
+  // too small for the mesh pays for its overflows.  Candidates: 128 or 256
+  // orientations per batch x the normal strip budget (four CTAs per SM, 72 KB,
+  // 99 KB) x the strip height (the planned one and half of it).  When most of
+  // the sample passes the 63-pixel cap in some column, every candidate starts
+  // in the priority-carrying strips (configuration 4), as an adaptive sweep
+  // would switch to them.
   int autotune(int sample, TuneResult* best)
   {
-    static const int kBatches[] = {64, 128, 256};
+    static const int kBatches[] = {128, 256};
     static const int kSmem[] = {0, 73728, 101376};   // 0: four CTAs per SM
-    best->batch = batch; best->normal_smem = normal_smem; best->us_per_orientation = 0.0;
+    best->batch = batch; best->normal_smem = normal_smem; best->strip_h = force_h; best->start_cfg = start_cfg;
+    best->us_per_orientation = 0.0;
     if (nYPR == 0 || P.n_tri == 0) return 0;
     const int n = std::min(nYPR, std::max(sample, 1));
     std::vector<int> ids(n);
@@ -1003,24 +1017,48 @@ struct Engine {
     TOMO_CUDA(cudaEventCreate(&b));
     const bool timing = log.timing;
     log.timing = false;
-    const int keep_batch = batch, keep_smem = normal_smem;
+    const int keep_batch = batch, keep_smem = normal_smem, keep_h = force_h, keep_cfg = start_cfg;
     double best_us = 1e300;
     int rc = 0;
+    // the planned strip height, and whether the sample is cap-heavy
+    plan_strips();
+    const int h_plan = cfg[0].H;
+    start_cfg = 0;
+    if ((rc = sweep_device(dids.ptr, n)) == 0) {
+      std::vector<int> fl(nYPR);
+      if (cudaStreamSynchronize(side) != cudaSuccess || cudaStreamSynchronize(main) != cudaSuccess ||
+          cudaMemcpy(fl.data(), o_flags.ptr, sizeof(int) * nYPR, cudaMemcpyDeviceToHost) != cudaSuccess)
+        rc = set_error(TOMO_ERR_CUDA, "autotune flags");
+      int capped = 0;
+      for (int i = 0; rc == 0 && i < n; i++) capped += (fl[ids[i]] & kFlagCap) ? 1 : 0;
+      if (rc == 0 && capped * 2 > n) start_cfg = 4;
+    }
+    const int tuned_cfg = start_cfg;
     for (int bsz : kBatches) {
-      for (int sm : kSmem) {
-        batch = bsz; normal_smem = sm;
-        plan_strips();
-        float ms = 0.f;
-        // an untimed run first: it allocates and warms
-        if ((rc = sweep_device(dids.ptr, n)) != 0) break;
-        if (cudaEventRecord(a, main) != cudaSuccess) { rc = set_error(TOMO_ERR_CUDA, "autotune event"); break; }
-        if ((rc = sweep_device(dids.ptr, n)) != 0) break;
-        if (cudaEventRecord(b, main) != cudaSuccess || cudaEventSynchronize(b) != cudaSuccess ||
-            cudaEventElapsedTime(&ms, a, b) != cudaSuccess) { rc = set_error(TOMO_ERR_CUDA, "autotune timing"); break; }
-        const double us = 1000.0 * ms / n;
-        if (us < best_us) { best_us = us; best->batch = bsz; best->normal_smem = sm; }
-      }
       if (rc) break;
+      for (int sm : kSmem) {
+        if (rc) break;
+        for (int h : {h_plan, h_plan / 2}) {
+          if (h < 1 || (h != h_plan && h_plan < 2)) continue;
+          batch = bsz; normal_smem = sm; force_h = (h == h_plan) ? keep_h : h;
+          plan_strips();
+          if (force_h && cfg[0].H != force_h) continue;   // the budget cannot hold that strip height
+          float ms = 0.f;
+          // an untimed run first: it allocates and warms
+          if ((rc = sweep_device(dids.ptr, n)) != 0) break;
+          if ((rc = resolve(&ids)) != 0) break;
+          if (cudaEventRecord(a, main) != cudaSuccess) { rc = set_error(TOMO_ERR_CUDA, "autotune event"); break; }
+          if ((rc = sweep_device(dids.ptr, n)) != 0) break;
+          if ((rc = resolve(&ids)) != 0) break;
+          if (cudaEventRecord(b, main) != cudaSuccess || cudaEventSynchronize(b) != cudaSuccess ||
+              cudaEventElapsedTime(&ms, a, b) != cudaSuccess) { rc = set_error(TOMO_ERR_CUDA, "autotune timing"); break; }
+          const double us = 1000.0 * ms / n;
+          if (us < best_us) {
+            best_us = us; best->batch = bsz; best->normal_smem = sm; best->strip_h = force_h;
+            best->start_cfg = tuned_cfg;
+          }
+        }
+      }
     }
     log.timing = timing;
     cudaStreamSynchronize(main);
@@ -1029,6 +1067,8 @@ struct Engine {
     dids.release();
     batch = rc ? keep_batch : best->batch;
     normal_smem = rc ? keep_smem : best->normal_smem;
+    force_h = rc ? keep_h : best->strip_h;
+    start_cfg = rc ? keep_cfg : best->start_cfg;
     plan_strips();
     best->us_per_orientation = best_us;
     return rc;
@@ -1865,7 +1905,8 @@ struct MultiEngine {
   int autotune = 1;
   int tune_sample = 512;
   int n_tuned = 0;
-  double last_ms = 0.0;
+  double last_ms = 0.0;        // last run: sweep and re-runs, until every mesh is resolved
+  double last_graph_ms = 0.0;  // last run: the sweep alone (graph replay)
 
   void clear_graph()
   {
@@ -1907,11 +1948,14 @@ struct MultiEngine {
       return (double)e.nYPR * ((double)e.P.n_tri + 0.25 * (double)e.G * (double)e.G);
     };
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost(a) > cost(b); });
-    choice.assign(n, Engine::TuneResult{128, 0, 0.0});
+    choice.assign(n, Engine::TuneResult{128, 0, 0, 0, 0.0});
     n_tuned = 0;
     for (int m = 0; m < n; m++) {
       Engine& e = *meshes[m];
-      if (!autotune || e.nYPR == 0 || e.P.n_tri == 0) { choice[m] = {e.batch, e.normal_smem, 0.0}; continue; }
+      if (!autotune || e.nYPR == 0 || e.P.n_tri == 0) {
+        choice[m] = {e.batch, e.normal_smem, e.force_h, e.start_cfg, 0.0};
+        continue;
+      }
       int t = 1;
       while (t < e.P.n_tri) t <<= 1;
       const std::pair<int, int> key((e.G + 31) / 32 * 32, t);
@@ -1924,6 +1968,8 @@ struct MultiEngine {
       }
       e.batch = it->second.batch;
       e.normal_smem = it->second.normal_smem;
+      e.force_h = it->second.strip_h;
+      e.start_cfg = it->second.start_cfg;
       e.plan_strips();
       choice[m] = it->second;
     }
@@ -2010,21 +2056,27 @@ struct MultiEngine {
           if ((rc = meshes[m]->sweep_device()) != 0) break;
       }
     }
-    float ms = 0.f;
+    // the sweep alone (graph) ends at g; the re-runs of flagged orientations
+    // follow per mesh on the same stream, and b marks every mesh resolved
+    cudaEvent_t g = nullptr;
+    if (rc == 0 && (cudaEventCreate(&g) != cudaSuccess || cudaEventRecord(g, W.main) != cudaSuccess))
+      rc = set_error(TOMO_ERR_CUDA, "event record");
+    for (auto* e : meshes)
+      if (rc == 0) rc = e->resolve();
+    float ms = 0.f, gms = 0.f;
     if (rc == 0) {
       if (cudaEventRecord(b, W.main) != cudaSuccess || cudaEventSynchronize(b) != cudaSuccess ||
-          cudaEventElapsedTime(&ms, a, b) != cudaSuccess)
+          cudaEventElapsedTime(&ms, a, b) != cudaSuccess || cudaEventElapsedTime(&gms, a, g) != cudaSuccess)
         rc = set_error(TOMO_ERR_CUDA, "batch timing");
     }
     cudaEventDestroy(a);
     cudaEventDestroy(b);
+    if (g) cudaEventDestroy(g);
     if (rc) return rc;
     last_ms = ms;
+    last_graph_ms = gms;
     if (device_ms) *device_ms = ms;
-    for (auto* e : meshes) {
-      TOMO_TRY(e->resolve());
-      e->finalize_host();
-    }
+    for (auto* e : meshes) e->finalize_host();
     return 0;
   }
 };
@@ -2082,9 +2134,10 @@ int tomoBatchStats(long long* out, int n)
   const MultiEngine& M = *g_multi;
   long long orient = 0, redo = 0;
   for (auto* e : M.meshes) { orient += e->nYPR; redo += e->n_redo[1] + e->n_redo[2] + e->n_redo[3] + e->n_redo[4]; }
-  const long long v[8] = {(long long)M.meshes.size(), orient, (long long)M.graph_nodes, M.graph_kernels,
-                          (long long)M.n_tuned, (long long)M.tuned.size(), redo, (long long)(M.last_ms * 1000.0)};
-  for (int k = 0; k < n && k < 8; k++) out[k] = v[k];
+  const long long v[9] = {(long long)M.meshes.size(), orient, (long long)M.graph_nodes, M.graph_kernels,
+                          (long long)M.n_tuned, (long long)M.tuned.size(), redo, (long long)(M.last_ms * 1000.0),
+                          (long long)(M.last_graph_ms * 1000.0)};
+  for (int k = 0; k < n && k < 9; k++) out[k] = v[k];
   return 0;
 }
 

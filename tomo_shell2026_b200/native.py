@@ -286,10 +286,10 @@ class Batch:
 
     @staticmethod
     def stats() -> dict:
-        out = np.zeros(8, np.int64)
-        _check(lib().tomoBatchStats(_p(out, _i64p), 8))
+        out = np.zeros(9, np.int64)
+        _check(lib().tomoBatchStats(_p(out, _i64p), 9))
         keys = ("meshes", "orientations", "graph_nodes", "graph_kernels", "tuned_now", "tuned_total", "reruns",
-                "device_us")
+                "device_us", "graph_us")
         return {k: int(v) for k, v in zip(keys, out)}
 
     @staticmethod
