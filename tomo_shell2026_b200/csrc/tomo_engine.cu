@@ -190,6 +190,10 @@ constexpr int kMaxGrid = 4096;
 // Orientations the last tomoSweepStatic call re-ran, per strip configuration.
 int g_static_reruns[5];
 
+// Proposal source of tomoSurrogateSearch: 0 the trained network, 1 bilinear
+// interpolation of the exact coarse values (the search without the network).
+int g_proposal = 0;
+
 struct BatchSet {   // per-batch buffers read by the fold, double-buffered
   DevBuf<long long> acc;
   DevBuf<int> flags;
@@ -1388,6 +1392,7 @@ int tomoSetOption(int key, int value)
     case TOMO_OPT_NORMAL_SMEM: if (value < 0 || value > 232448) return TOMO_ERR_ARG; E.normal_smem = value; return 0;
     case TOMO_OPT_EXPORT: E.export_pixels = value ? 1 : 0; return 0;
     case TOMO_OPT_ADAPTIVE: E.adaptive = value ? 1 : 0; E.adapt_smem = E.adapt_h = E.adapt_cfg = 0; return 0;
+    case TOMO_OPT_PROPOSAL: if (value < 0 || value > 1) return TOMO_ERR_ARG; g_proposal = value; return 0;
     default: return TOMO_ERR_ARG;
   }
 }
@@ -2390,69 +2395,94 @@ int tomoSurrogateSearch(const float* f32info, const int* i32info, const float* Y
       for (int iy = 0; iy < n_yaw; iy += stride) coarse.push_back(ip * n_yaw + iy);
     n_coarse = (int)coarse.size();
     TOMO_TRY(evaluate(coarse));
-    // 2. features of every grid point on the device (the same bits for
-    //    training and prediction); a seeded share of the coarse points is
-    //    held out of training so the prediction error is also measured away
-    //    from the refined cells; train on standardised exact Vss
-    DevBuf<float> dypr, dx, dy;
-    TOMO_CUDA(dypr.reserve((size_t)n * 3));
-    TOMO_CUDA(dx.reserve((size_t)n * kMlpIn));
-    TOMO_CUDA(dy.reserve((size_t)n));
-    TOMO_CUDA(cudaMemcpyAsync(dypr.ptr, YPR, sizeof(float) * n * 3, cudaMemcpyHostToDevice, E.main));
-    TOMO_CUDA(mlp_features(dypr.ptr, n, dx.ptr, E.main));
-    std::vector<float> F((size_t)n * kMlpIn);
-    TOMO_CUDA(cudaMemcpyAsync(F.data(), dx.ptr, sizeof(float) * F.size(), cudaMemcpyDeviceToHost, E.main));
-    TOMO_CUDA(cudaStreamSynchronize(E.main));
-    std::vector<int> train;
-    {
-      unsigned h = 2166136261u ^ (unsigned)seed;
-      for (int id : coarse) {
-        h = (h ^ (unsigned)id) * 16777619u;   // FNV-1a step: a fixed pseudo-random split
-        const float u = (float)((h >> 8) & 0xFFFF) / 65536.f;
-        if (u >= holdout) { train.push_back(id); trained[id] = 1; }
+    if (g_proposal == 1) {
+      // 2'-3'. the search without the network: the exact coarse Vss,
+      // bilinearly interpolated onto every grid point (yaw wraps around);
+      // the coarse points are exact, so the error is measured on the
+      // refined points only
+      const auto t0 = std::chrono::steady_clock::now();
+      const int ncyc = (n_yaw + stride - 1) / stride, ncpc = (n_pitch + stride - 1) / stride;
+      auto cval = [&](int p, int y) { return (double)E.vss64[(size_t)(p * stride) * n_yaw + (size_t)(y * stride)]; };
+      for (int ip = 0; ip < n_pitch; ip++) {
+        const double fp = std::min((double)ip / stride, (double)(ncpc - 1));
+        const int p0 = (int)std::floor(fp), p1 = std::min(p0 + 1, ncpc - 1);
+        const double wp = fp - p0;
+        for (int iy = 0; iy < n_yaw; iy++) {
+          const double fy = (double)iy / stride;
+          const int y0 = (int)std::floor(fy) % ncyc, y1 = (y0 + 1) % ncyc;
+          const double wy = fy - std::floor(fy);
+          const double r0 = cval(p0, y0) * (1.0 - wy) + cval(p0, y1) * wy;
+          const double r1 = cval(p1, y0) * (1.0 - wy) + cval(p1, y1) * wy;
+          pred[(size_t)ip * n_yaw + iy] = (float)((1.0 - wp) * r0 + wp * r1);
+        }
       }
-      if (train.empty()) { train = coarse; for (int id : coarse) trained[id] = 1; }
-    }
-    // target: Vss, or with log_scale > 0 log1p((Vss - min) / s), s = log_scale x
-    // (median - min) of the training Vss, which spends the network's accuracy
-    // near the minimum; then standardised
-    std::vector<double> tv;
-    for (int id : train) tv.push_back((double)E.vss64[id]);
-    std::vector<double> sorted_tv = tv;
-    std::sort(sorted_tv.begin(), sorted_tv.end());
-    const double vmin = sorted_tv.front();
-    const double tscale = log_scale > 0.f ? std::max(1.0, (double)log_scale * (sorted_tv[sorted_tv.size() / 2] - vmin)) : 0.0;
-    auto fwd = [&](double v) { return tscale > 0.0 ? std::log1p((v - vmin) / tscale) : v; };
-    auto inv = [&](double y) { return tscale > 0.0 ? vmin + tscale * std::expm1(y) : y; };
-    double mean = 0.0, sq = 0.0;
-    for (double v : tv) mean += fwd(v);
-    mean /= (double)tv.size();
-    for (double v : tv) sq += (fwd(v) - mean) * (fwd(v) - mean);
-    const double sd = tv.size() > 1 && sq > 0.0 ? std::sqrt(sq / (double)tv.size()) : 1.0;
-    std::vector<float> X(train.size() * kMlpIn), Y(train.size());
-    for (size_t k = 0; k < train.size(); k++) {
-      std::memcpy(&X[k * kMlpIn], &F[(size_t)train[k] * kMlpIn], sizeof(float) * kMlpIn);
-      Y[k] = (float)((fwd(tv[k]) - mean) / sd);
-    }
-    {
-      const auto t0 = std::chrono::steady_clock::now();
-      TOMO_CUDA(mlp().init((unsigned)seed, E.main));
-      TOMO_CUDA(mlp().set_data(X.data(), Y.data(), (int)train.size(), E.main));
-      TOMO_CUDA(mlp().fit(steps, lr, E.main, &train_loss));
-      t_train += seconds_since(t0);
-    }
-    // 3. predict every grid point
-    {
-      const auto t0 = std::chrono::steady_clock::now();
-      TOMO_CUDA(mlp().predict_device(dx.ptr, n, dy.ptr, E.main));
-      TOMO_CUDA(cudaMemcpyAsync(pred.data(), dy.ptr, sizeof(float) * n, cudaMemcpyDeviceToHost, E.main));
-      TOMO_CUDA(cudaStreamSynchronize(E.main));
-      for (int id = 0; id < n; id++) pred[id] = (float)inv(pred[id] * sd + mean);
+      for (int id : coarse) trained[id] = 1;
       t_pred += seconds_since(t0);
+    } else {
+      // 2. features of every grid point on the device (the same bits for
+      //    training and prediction); a seeded share of the coarse points is
+      //    held out of training so the prediction error is also measured away
+      //    from the refined cells; train on standardised exact Vss
+      DevBuf<float> dypr, dx, dy;
+      TOMO_CUDA(dypr.reserve((size_t)n * 3));
+      TOMO_CUDA(dx.reserve((size_t)n * kMlpIn));
+      TOMO_CUDA(dy.reserve((size_t)n));
+      TOMO_CUDA(cudaMemcpyAsync(dypr.ptr, YPR, sizeof(float) * n * 3, cudaMemcpyHostToDevice, E.main));
+      TOMO_CUDA(mlp_features(dypr.ptr, n, dx.ptr, E.main));
+      std::vector<float> F((size_t)n * kMlpIn);
+      TOMO_CUDA(cudaMemcpyAsync(F.data(), dx.ptr, sizeof(float) * F.size(), cudaMemcpyDeviceToHost, E.main));
+      TOMO_CUDA(cudaStreamSynchronize(E.main));
+      std::vector<int> train;
+      {
+        unsigned h = 2166136261u ^ (unsigned)seed;
+        for (int id : coarse) {
+          h = (h ^ (unsigned)id) * 16777619u;   // FNV-1a step: a fixed pseudo-random split
+          const float u = (float)((h >> 8) & 0xFFFF) / 65536.f;
+          if (u >= holdout) { train.push_back(id); trained[id] = 1; }
+        }
+        if (train.empty()) { train = coarse; for (int id : coarse) trained[id] = 1; }
+      }
+      // target: Vss, or with log_scale > 0 log1p((Vss - min) / s), s = log_scale x
+      // (median - min) of the training Vss, which spends the network's accuracy
+      // near the minimum; then standardised
+      std::vector<double> tv;
+      for (int id : train) tv.push_back((double)E.vss64[id]);
+      std::vector<double> sorted_tv = tv;
+      std::sort(sorted_tv.begin(), sorted_tv.end());
+      const double vmin = sorted_tv.front();
+      const double tscale = log_scale > 0.f ? std::max(1.0, (double)log_scale * (sorted_tv[sorted_tv.size() / 2] - vmin)) : 0.0;
+      auto fwd = [&](double v) { return tscale > 0.0 ? std::log1p((v - vmin) / tscale) : v; };
+      auto inv = [&](double y) { return tscale > 0.0 ? vmin + tscale * std::expm1(y) : y; };
+      double mean = 0.0, sq = 0.0;
+      for (double v : tv) mean += fwd(v);
+      mean /= (double)tv.size();
+      for (double v : tv) sq += (fwd(v) - mean) * (fwd(v) - mean);
+      const double sd = tv.size() > 1 && sq > 0.0 ? std::sqrt(sq / (double)tv.size()) : 1.0;
+      std::vector<float> X(train.size() * kMlpIn), Y(train.size());
+      for (size_t k = 0; k < train.size(); k++) {
+        std::memcpy(&X[k * kMlpIn], &F[(size_t)train[k] * kMlpIn], sizeof(float) * kMlpIn);
+        Y[k] = (float)((fwd(tv[k]) - mean) / sd);
+      }
+      {
+        const auto t0 = std::chrono::steady_clock::now();
+        TOMO_CUDA(mlp().init((unsigned)seed, E.main));
+        TOMO_CUDA(mlp().set_data(X.data(), Y.data(), (int)train.size(), E.main));
+        TOMO_CUDA(mlp().fit(steps, lr, E.main, &train_loss));
+        t_train += seconds_since(t0);
+      }
+      // 3. predict every grid point
+      {
+        const auto t0 = std::chrono::steady_clock::now();
+        TOMO_CUDA(mlp().predict_device(dx.ptr, n, dy.ptr, E.main));
+        TOMO_CUDA(cudaMemcpyAsync(pred.data(), dy.ptr, sizeof(float) * n, cudaMemcpyDeviceToHost, E.main));
+        TOMO_CUDA(cudaStreamSynchronize(E.main));
+        for (int id = 0; id < n; id++) pred[id] = (float)inv(pred[id] * sd + mean);
+        t_pred += seconds_since(t0);
+      }
+      dypr.release();
+      dx.release();
+      dy.release();
     }
-    dypr.release();
-    dx.release();
-    dy.release();
     // 4. cells by smallest prediction; refine the top_k
     std::vector<float> cmin(ncell, INFINITY);
     for (int id = 0; id < n; id++) { const int c = cell_of(id); cmin[c] = std::min(cmin[c], pred[id]); }

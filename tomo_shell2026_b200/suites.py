@@ -117,50 +117,80 @@ def coarse_interpolation(vss: np.ndarray, n_yaw: int, n_pitch: int, stride: int)
 
 def surrogate_suite(n_meshes: int = 100, seed0: int = 1000, stride: int = 10, cell: int = 5, top_k: int = 64,
                     steps: int = 300, ratio_target: float = 0.2, margin: float = 1.0, holdout: float = 0.0,
-                    lr: float = 3e-3, max_eval: int = -1, log_scale: float = 0.3) -> dict:
+                    lr: float = 3e-3, max_eval: int = -1, log_scale: float = 0.3, ablation: bool = True) -> dict:
+    """The learned-proposal search against the exhaustive sweep on the same
+    meshes, and (``ablation``) the same search without the network -- blocks
+    ranked by a bilinear interpolation of the exact coarse values -- so the
+    network's gain is measured on identical inputs.
+
+    Clocks: ``exhaustive_s`` is device time (CUDA events on the library's
+    stream around tomoSweepDevice: the whole 0.5-degree sweep, re-runs and
+    result fetch, mesh already uploaded); ``search_s`` is host wall-clock time
+    around the tomoSurrogateSearch call (upload, coarse sweep, training,
+    prediction, refinement rounds, result fetch)."""
     ypr = meshgen.ypr_grid(np.arange(0, 360, 0.5), np.arange(0, 60.5, 0.5))
     n_yaw, n_pitch = 720, 121
     opts = PrintOptions(explicit_ss=True)
+    kw = dict(stride=stride, cell=cell, top_k=top_k, steps=steps, margin=margin, holdout=holdout, lr=lr,
+              max_eval=max_eval, log_scale=log_scale)
+    kinds = ("network", "interpolation") if ablation else ("network",)
     rows = []
-    # one untimed search first: first-call costs (allocations, kernel loading)
+    # one untimed search of each kind first: first-call costs (allocations, kernel loading)
     warm = meshgen.small_solid(seed0 - 1, with_hull=False)
-    surrogate.search(warm, ypr, n_yaw, n_pitch, opts, stride=stride, cell=cell, top_k=top_k, steps=steps,
-                     margin=margin, holdout=holdout, lr=lr, max_eval=max_eval, log_scale=log_scale)
+    for kind in kinds:
+        surrogate.search(warm, ypr, n_yaw, n_pitch, opts, proposal=kind, **kw)
     for k in range(n_meshes):
         m = meshgen.small_solid(seed0 + k, with_hull=False)
         s = native.Session(m, ypr, opts)
         s.run_device()
         ex_s = s.run_device() / 1000.0
         opt, _, mss, _ = s.finish()
-        vss = native.results(ypr.shape[0])["Vss64"]
-        r = surrogate.search(m, ypr, n_yaw, n_pitch, opts, stride=stride, cell=cell, top_k=top_k, steps=steps,
-                             seed=k, margin=margin, holdout=holdout, lr=lr, max_eval=max_eval, log_scale=log_scale)
-        rows.append(dict(same_value=bool(np.float32(r.Mss[r.optID]) == mss[opt]), same_index=r.optID == opt,
-                         ratio=r.seconds / ex_s, exhaustive_s=ex_s, search_s=r.seconds, evaluated=r.evaluated,
-                         fallback=r.fallback, rel_error=r.rel_error,
-                         rank_network=block_rank(r.pred_vss, opt, n_yaw, n_pitch, cell),
-                         rank_without=block_rank(coarse_interpolation(vss, n_yaw, n_pitch, stride), opt, n_yaw,
-                                                 n_pitch, cell)))
-    ok = [x["same_value"] and x["ratio"] <= ratio_target for x in rows]
-    return {"meshes": n_meshes, "grid": [n_yaw, n_pitch], "orientations": int(ypr.shape[0]),
-            "coarse_deg": stride * 0.5, "cell_deg": cell * 0.5, "margin": margin, "holdout": holdout,
-            "train_steps": steps, "learning_rate": lr, "max_eval": max_eval, "log_scale": log_scale,
-            "optimum_recall": float(np.mean([x["same_value"] for x in rows])),
-            "same_index": float(np.mean([x["same_index"] for x in rows])),
-            "fallbacks": int(sum(x["fallback"] for x in rows)),
-            "median_time_ratio": float(np.median([x["ratio"] for x in rows])),
-            "p95_time_ratio": float(np.percentile([x["ratio"] for x in rows], 95)),
-            "meshes_at_target": float(np.mean(ok)), "ratio_target": ratio_target,
-            "median_exhaustive_s": float(np.median([x["exhaustive_s"] for x in rows])),
-            "median_search_s": float(np.median([x["search_s"] for x in rows])),
-            "median_evaluated": float(np.median([x["evaluated"] for x in rows])),
-            "median_rel_error": float(np.median([x["rel_error"] for x in rows])),
-            # where the optimum's block lands when blocks are ranked by the
-            # network versus by interpolating the exact coarse values
-            "optimum_block_in_top_k_network": float(np.mean([x["rank_network"] < top_k for x in rows])),
-            "optimum_block_in_top_k_without_network": float(np.mean([x["rank_without"] < top_k for x in rows])),
-            "median_optimum_block_rank_network": float(np.median([x["rank_network"] for x in rows])),
-            "median_optimum_block_rank_without_network": float(np.median([x["rank_without"] for x in rows]))}
+        row = dict(exhaustive_s=ex_s)
+        for kind in kinds:
+            r = surrogate.search(m, ypr, n_yaw, n_pitch, opts, seed=k, proposal=kind, **kw)
+            row[kind] = dict(same_value=bool(np.float32(r.Mss[r.optID]) == mss[opt]), same_index=r.optID == opt,
+                             ratio=r.seconds / ex_s, search_s=r.seconds, evaluated=r.evaluated,
+                             fallback=r.fallback, rel_error=r.rel_error, max_abs_error=r.max_abs_error,
+                             rank=block_rank(r.pred_vss, opt, n_yaw, n_pitch, cell))
+        rows.append(row)
+
+    def summary(kind):
+        xs = [r[kind] for r in rows]
+        ok = [x["same_value"] and x["ratio"] <= ratio_target for x in xs]
+        return {"optimum_recall": float(np.mean([x["same_value"] for x in xs])),
+                "same_index": float(np.mean([x["same_index"] for x in xs])),
+                "fallbacks": int(sum(x["fallback"] for x in xs)),
+                "meshes_at_target": float(np.mean(ok)),
+                "median_time_ratio": float(np.median([x["ratio"] for x in xs])),
+                "p95_time_ratio": float(np.percentile([x["ratio"] for x in xs], 95)),
+                "median_search_s": float(np.median([x["search_s"] for x in xs])),
+                "median_evaluated": float(np.median([x["evaluated"] for x in xs])),
+                "mean_evaluated": float(np.mean([x["evaluated"] for x in xs])),
+                "median_rel_error": float(np.median([x["rel_error"] for x in xs])),
+                "median_max_abs_error": float(np.median([x["max_abs_error"] for x in xs])),
+                "optimum_block_in_top_k": float(np.mean([x["rank"] < top_k for x in xs])),
+                "median_optimum_block_rank": float(np.median([x["rank"] for x in xs])),
+                "mean_optimum_block_rank": float(np.mean([x["rank"] for x in xs]))}
+
+    out = {"meshes": n_meshes, "grid": [n_yaw, n_pitch], "orientations": int(ypr.shape[0]),
+           "coarse_deg": stride * 0.5, "cell_deg": cell * 0.5, "margin": margin, "holdout": holdout,
+           "train_steps": steps, "learning_rate": lr, "max_eval": max_eval, "log_scale": log_scale,
+           "ratio_target": ratio_target,
+           "median_exhaustive_s": float(np.median([r["exhaustive_s"] for r in rows])),
+           "clocks": {"exhaustive": "device time, CUDA events around tomoSweepDevice (sweep, re-runs, result fetch)",
+                      "search": "host wall clock around tomoSurrogateSearch (everything from upload to results)"}}
+    out.update(summary("network"))
+    if ablation:
+        out["without_network"] = summary("interpolation")
+        ev_net = np.array([r["network"]["evaluated"] for r in rows], np.float64)
+        ev_wo = np.array([r["interpolation"]["evaluated"] for r in rows], np.float64)
+        out["network_gain"] = {
+            "evaluations_saved_mean": float(np.mean(ev_wo - ev_net)),
+            "evaluations_ratio_median": float(np.median(ev_net / np.maximum(ev_wo, 1))),
+            "meshes_fewer_evaluations": float(np.mean(ev_net < ev_wo)),
+            "time_ratio_median": float(np.median([r["network"]["search_s"] / r["interpolation"]["search_s"]
+                                                  for r in rows]))}
+    return out
 
 
 def shell_suite(seed: int = 0) -> dict:

@@ -88,14 +88,22 @@ class SearchResult:
 
 def search(mesh, ypr, n_yaw: int, n_pitch: int, opts, stride: int = 10, cell: int = 5, top_k: int = 64,
            steps: int = 300, lr: float = 3e-3, seed: int = 0, max_eval: int = -1, gate: float = 0.5,
-           margin: float = 1.0, holdout: float = 0.0, log_scale: float = 0.3) -> SearchResult:
+           margin: float = 1.0, holdout: float = 0.0, log_scale: float = 0.3,
+           proposal: str = "network") -> SearchResult:
     """Learned-proposal search over ypr = grid [n_pitch][n_yaw] (yaw fastest):
     coarse training points every `stride` grid steps, refinement in blocks of
     cell x cell grid points, fallback past max_eval evaluated orientations
     (default: an eighth of the grid); see tomoSurrogateSearch.  The defaults
     are the setting measured on the 0.5-degree grid with 5-degree coarse
-    points: 64 proposed 2.5-degree blocks, log-scaled targets, margin 1."""
+    points: 64 proposed 2.5-degree blocks, log-scaled targets, margin 1.
+
+    ``proposal="interpolation"`` runs the same search without the network:
+    the blocks are ranked by a bilinear interpolation of the exact coarse
+    values and the error gate uses that interpolation's observed error."""
+    from .native import TOMO_OPT_PROPOSAL
     from .options import pack_info
+    if proposal not in ("network", "interpolation"):
+        raise ValueError("proposal must be 'network' or 'interpolation'")
     f32, i32 = pack_info(opts, mesh, ypr.shape[0])
     ypr, tri, vtx, vn, *_ = _arrays(mesh, ypr)
     n = ypr.shape[0]
@@ -106,8 +114,13 @@ def search(mesh, ypr, n_yaw: int, n_pitch: int, opts, stride: int = 10, cell: in
     mss = np.zeros(n, np.float32)
     pred = np.zeros(n, np.float32)
     st = np.zeros(12, np.float64)
-    opt = _check(_lib().tomoSurrogateSearch(_p(f32, _f32p), _p(i32, _i32p), _p(ypr, _f32p), _p(tri, _i32p),
-                                            _p(vtx, _f32p), _p(vn, _f32p), int(n_yaw), int(n_pitch), _p(ip, _i32p),
-                                            _p(fp, _f32p), _p(mss, _f32p), _p(pred, _f32p), st.ctypes.data_as(_f64p)))
+    _check(_lib().tomoSetOption(TOMO_OPT_PROPOSAL, 1 if proposal == "interpolation" else 0))
+    try:
+        opt = _check(_lib().tomoSurrogateSearch(_p(f32, _f32p), _p(i32, _i32p), _p(ypr, _f32p), _p(tri, _i32p),
+                                                _p(vtx, _f32p), _p(vn, _f32p), int(n_yaw), int(n_pitch),
+                                                _p(ip, _i32p), _p(fp, _f32p), _p(mss, _f32p), _p(pred, _f32p),
+                                                st.ctypes.data_as(_f64p)))
+    finally:
+        _lib().tomoSetOption(TOMO_OPT_PROPOSAL, 0)
     return SearchResult(opt, mss, pred, int(st[0]), bool(st[1]), float(st[2]), float(st[3]), float(st[4]),
                         float(st[5]), float(st[6]), float(st[7]), float(st[8]), int(st[9]), int(st[10]), int(st[11]))
