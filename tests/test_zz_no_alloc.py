@@ -86,14 +86,36 @@ def test_static_rerun_ladder_first_come_cap():
         assert _static_reruns()[1] > 0, "no orientation took the priority re-run"
 
 
-def test_static_rerun_ladder_dense_mesh():
-    """A dense 16k-triangle sphere (about one triangle per voxel face): strip
-    lists and silhouette columns force re-runs; results equal TomoSh_CUDA's."""
+def _wide_layers(n_layers=20, n=20, seed=4):
+    """Stacked wavy sheets across most of the 256-column grid: about twenty
+    pixels in every column, far more entries per strip than a default strip
+    holds."""
+    rng = np.random.default_rng(seed)
+    V, F = [], []
+    for L in range(n_layers):
+        xs, ys = np.meshgrid(np.linspace(20, 170, n), np.linspace(20, 170, n), indexing="ij")
+        zs = 10 + L * 2.3 + 0.8 * np.sin(xs * 0.3 + L) + 0.5 * rng.standard_normal(xs.shape)
+        base = len(V)
+        V += list(np.stack([xs.ravel(), ys.ravel(), zs.ravel()], 1))
+        for i in range(n - 1):
+            for j in range(n - 1):
+                a = base + i * n + j
+                b, c, d = a + 1, a + n, a + n + 1
+                F += [(a, c, b), (b, c, d)] if L % 2 else [(a, b, c), (b, d, c)]
+    return meshgen.mesh_from_arrays(np.array(V), np.array(F), "wide_layers", with_hull=False)
+
+
+def test_static_rerun_ladder_overflowing_strips():
+    """Strips whose pixel lists overflow the default shared-memory budget are
+    re-run with the large budget (and beyond that in safe mode), as
+    TomoSh_CUDA does; results equal TomoSh_CUDA's, twice."""
     _defaults()
-    mesh = meshgen.perturbed_sphere(16000, 30.0, 7, with_hull=False)
-    ypr = meshgen.ypr_grid(np.arange(0, 360, 45), np.arange(0, 61, 30))
+    mesh = _wide_layers()
+    assert mesh.n_tri <= 16384
+    ypr = meshgen.ypr_grid(np.arange(0, 360, 90), np.arange(0, 61, 30))
     opts = PrintOptions()
     ref = native.sweep(mesh, ypr, opts)
     for _ in range(2):
         _same(ref, native.sweep_static(mesh, ypr, opts))
-    assert sum(_static_reruns()) > 0, "the dense mesh re-ran nothing"
+        big, prio, safe = _static_reruns()
+        assert big + safe > 0, "no strip overflowed"

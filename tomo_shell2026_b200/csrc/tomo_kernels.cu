@@ -447,6 +447,7 @@ __global__ void __launch_bounds__(256) k_bin_fill(EngineParams p)
 constexpr int kChunk = 256;    // triangles staged per pass (== blockDim.x)
 constexpr int kRegKeys = 8;    // columns with up to this many raw pixels sort in registers
 constexpr int kMaxEnt = 32767; // entry indices are stored as int16
+constexpr int kWarpKeys = 64;  // raw entries a warp sorts in registers (two per lane)
 
 struct StripSmem {
   int* heads;          // [H*G] first entry of each column list, -1 if empty
@@ -461,8 +462,11 @@ struct StripSmem {
   int* pref;           // [kChunk + 4]
   unsigned* thit;      // [kChunk / 32] triangles with an accepted pixel
   uint8_t* tkind;      // [kChunk] bit 0: fallback only; bit 1: box inside one strip
+  float* fbz;          // [kChunk] z of each staged triangle's centroid fallback pixel
   short* olist;        // [H*G] occupied local slots in slot order (aliases the chunk area)
   short* longq;        // [H*G] phase B: positions in olist of columns with three or more raw entries
+  short* longq2;       // [H*G] phase B, normal strips: columns of more than kRegKeys raw entries
+  unsigned* wbuf;      // [warps][kWarpKeys] phase B, normal strips: one long column's keys per warp
   unsigned* scr;       // phase B: per-thread key scratch, scr[i * blockDim + thread] (chunk area after longq)
   int scr_cap;         // keys per thread in scr
 };
@@ -470,7 +474,7 @@ struct StripSmem {
 __host__ __device__ inline size_t strip_chunk_bytes()
 {
   return 3 * sizeof(float4) * kChunk + sizeof(int4) * kChunk + sizeof(int) * (kChunk + 4) + sizeof(unsigned) * (kChunk / 32) +
-         kChunk;
+         sizeof(float) * kChunk + kChunk;
 }
 
 __host__ __device__ inline size_t round16(size_t b) { return (b + 15) / 16 * 16; }
@@ -483,7 +487,10 @@ __host__ __device__ inline size_t strip_smem_layout(int mode, int H, int G, int 
   b += round16(sizeof(unsigned) * (size_t)C) + round16(sizeof(short) * (size_t)C);
   if (mode != 0) b += 2 * round16(sizeof(unsigned) * (size_t)C) + round16((size_t)C);
   const size_t chunk = strip_chunk_bytes();
-  const size_t olist = 2 * round16(sizeof(short) * HG);   // occupied-slot list + long-column queue
+  // phase B: occupied-slot list + long-column queue (+ normal strips: the queue of
+  // columns past kRegKeys raw entries and the per-warp key buffers)
+  const size_t ob = round16(sizeof(short) * HG);
+  const size_t olist = mode == 0 ? 3 * ob + sizeof(unsigned) * kWarpKeys * (kChunk / 32) : 2 * ob;
   return b + (chunk > olist ? chunk : olist);
 }
 
@@ -598,6 +605,69 @@ __device__ __forceinline__ bool column_short(const EngineParams& p, const StripS
   if (dump) { dump_key(p, gslot, 0, hi, t0); dump_key(p, gslot, 1, lo, t1); }
   col_result(p, s, 2, r);
   return true;
+}
+
+// Column stage of a normal-strip column of more than kRegKeys and at most
+// kWarpKeys raw entries, by one warp: lane 0 copies the list into the warp's
+// key buffer, every lane ranks its two keys among the distinct keys (first
+// occurrences) with shuffles, the distinct keys are scattered into
+// descending order, and lane 0 runs the column scan (col_step) over them --
+// the per-thread path's result, without its per-key list walks.  More than
+// 63 distinct keys flag the orientation for first-come priorities, as the
+// per-thread path does.  Every lane returns lane 0's result.
+__device__ __forceinline__ void column_warp(const EngineParams& p, const StripSmem& sm, int head, int n,
+                                            unsigned* wbuf, bool dump, int gslot, int* sflag, ColOut& r)
+{
+  const int lane = threadIdx.x & 31;
+  if (lane == 0) {
+    int m = 0;
+    for (int e = head; e >= 0 && m < kWarpKeys; e = sm.enext[e]) wbuf[m++] = sm.ekey[e];
+  }
+  __syncwarp();
+  const bool va = lane < n, vb = lane + 32 < n;
+  const unsigned ka = va ? wbuf[lane] : 0u, kb = vb ? wbuf[lane + 32] : 0u;
+  // first occurrences: no equal key at a smaller list position
+  bool fa = va, fb = vb;
+  for (int j = 0; j < 32; j++) {
+    const unsigned x = __shfl_sync(0xFFFFFFFFu, ka, j), y = __shfl_sync(0xFFFFFFFFu, kb, j);
+    if (j < n) { fa = fa && !(x == ka && j < lane); fb = fb && !(x == kb); }
+    if (j + 32 < n) fb = fb && !(y == kb && j < lane);
+  }
+  // rank among the distinct keys, descending
+  int ra = 0, rb = 0;
+  for (int j = 0; j < 32; j++) {
+    const unsigned x = __shfl_sync(0xFFFFFFFFu, ka, j), y = __shfl_sync(0xFFFFFFFFu, kb, j);
+    const bool fx = __shfl_sync(0xFFFFFFFFu, fa, j), fy = __shfl_sync(0xFFFFFFFFu, fb, j);
+    ra += (fx && x > ka) + (fy && y > ka);
+    rb += (fx && x > kb) + (fy && y > kb);
+  }
+  const int d = __popc(__ballot_sync(0xFFFFFFFFu, fa)) + __popc(__ballot_sync(0xFFFFFFFFu, fb));
+  r.vo = r.vss = r.tc = 0; r.ndist = 0; r.nfin = 0; r.lastz = 0; r.lasttype = 0; r.has10 = 0;
+  if (d > kSlotCap) {   // first-come order decides which keys survive
+    if (lane == 0) atomicOr(sflag, kFlagCap);
+    return;
+  }
+  __syncwarp();
+  if (fa) wbuf[ra] = ka;
+  if (fb) wbuf[rb] = kb;
+  __syncwarp();
+  if (lane == 0) {
+    if (d == 1) {   // duplicates of a single key
+      r.ndist = 1; r.nfin = 1; r.lastz = key_z(wbuf[0]); r.lasttype = 0;
+      r.has10 = (key_z(wbuf[0]) == 1 && key_nz(wbuf[0]) == 0);
+      if (dump) dump_key(p, gslot, 0, wbuf[0], 0);
+    } else {
+      ColState s;
+      col_init(s);
+      for (int i = 0; i < d; i++) {
+        const unsigned key = wbuf[i];
+        const int t = col_step(s, key_z(key), key_nz(key), p.thr, p.explicit_ss);
+        if (dump) dump_key(p, gslot, i, key, t);
+      }
+      col_result(p, s, d, r);
+    }
+  }
+  __syncwarp();
 }
 
 // Column stage of one slot from its shared-memory list.
@@ -844,7 +914,7 @@ template <int MODE>
 __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 1) k_strip(EngineParams p)
 {
   extern __shared__ __align__(16) unsigned char smem[];
-  __shared__ int nent, sflag, nlong, wtot[32];
+  __shared__ int nent, sflag, nlong, nlong2, wtot[32];
   __shared__ long long red[8][8];
 
   const int s = blockIdx.x, o = blockIdx.y;
@@ -875,6 +945,7 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 1) k_strip(EngineParams p
   sm.tm = (int4*)q; q += sizeof(int4) * kChunk;
   sm.pref = (int*)q; q += sizeof(int) * (kChunk + 4);
   sm.thit = (unsigned*)q; q += sizeof(unsigned) * (kChunk / 32);
+  sm.fbz = (float*)q; q += sizeof(float) * kChunk;
   sm.tkind = (uint8_t*)q; q += kChunk;
   sm.olist = (short*)chunk;
 
@@ -906,12 +977,27 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 1) k_strip(EngineParams p
     const int i = threadIdx.x;
     const int nchunk = min(kChunk, nlist - cb);
     int npix = 0;
+    // centroid fallback pixel of this thread's triangle (STomoSh_INT3.cpp:1190-1206), from the
+    // translated unmargined vertices while they are in registers; used after the walk if the
+    // triangle had no accepted pixel: slot x, y packed as two int16 (normal strips keep them in
+    // the staged triangle record, whose triangle index only priority strips read), and z (fbz)
+    int fb_xy = 0;
     if (i < nchunk) {
       const int entry = list[cb + i];
       const int t = entry & 0x7FFFFFFF;
       const int fb_only = (entry < 0) ? 1 : 0;
       TriGeo g;
-      load_tri(p, o, t, sh, g);
+      float4 raw[3];
+      load_tri(p, o, t, sh, g, raw);
+      {
+        const int sx = __float2int_rz(centroid(__fsub_rn(raw[0].x, sh.dx), __fsub_rn(raw[1].x, sh.dx),
+                                               __fsub_rn(raw[2].x, sh.dx)));
+        const int sy = __float2int_rz(centroid(__fsub_rn(raw[0].y, sh.dy), __fsub_rn(raw[1].y, sh.dy),
+                                               __fsub_rn(raw[2].y, sh.dy)));
+        // clamped into int16 first: anything outside [0, G) stays outside it and is flagged by emit
+        fb_xy = (min(max(sx, -1), 32767) & 0xFFFF) | (min(max(sy, -1), 32767) << 16);
+        sm.fbz[i] = centroid(__fsub_rn(raw[0].z, sh.dz), __fsub_rn(raw[1].z, sh.dz), __fsub_rn(raw[2].z, sh.dz));
+      }
       Bary b;
       bary_setup(g, b);
       int xc0, xc1;
@@ -924,7 +1010,7 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 1) k_strip(EngineParams p
       sm.q0[i] = make_float4(g.ax, g.ay, g.az, g.n0);
       sm.q1[i] = make_float4(g.bx, g.by, g.bz, g.n1);
       sm.q2[i] = make_float4(g.cx, g.cy, g.cz, g.n2);
-      sm.tm[i] = make_int4(t, g.x0, g.y0, ylen);
+      sm.tm[i] = make_int4(MODE == 0 ? fb_xy : t, g.x0, g.y0, ylen);
       sm.tkind[i] = (uint8_t)(fb_only | (single << 1));
     }
     if (i < kChunk / 32) sm.thit[i] = 0u;
@@ -1019,19 +1105,14 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 1) k_strip(EngineParams p
       const bool fb = (kind & 1) || ((kind & 2) && ((sm.thit[i >> 5] >> (i & 31)) & 1u) == 0u);
       if (fb) {
         const float n0 = sm.q0[i].w;
-        const unsigned t = (unsigned)sm.tm[i].x;
-        // centroid of the translated (unmargined) vertices, reloaded: few triangles take this path
-        const int4 ix = p.tri[t];
-        const float4* X = p.xf + (size_t)o * p.nV;
-        const float4 A = X[ix.x], B = X[ix.y], Cv = X[ix.z];
-        const float3 c3 = make_float3(
-            centroid(__fsub_rn(A.x, sh.dx), __fsub_rn(B.x, sh.dx), __fsub_rn(Cv.x, sh.dx)),
-            centroid(__fsub_rn(A.y, sh.dy), __fsub_rn(B.y, sh.dy), __fsub_rn(Cv.y, sh.dy)),
-            centroid(__fsub_rn(A.z, sh.dz), __fsub_rn(B.z, sh.dz), __fsub_rn(Cv.z, sh.dz)));
-        const int sx = __float2int_rz(c3.x), sy = __float2int_rz(c3.y);
-        emit<MODE>(p, sm, &nent, &sflag, xs0, xs1, sx, sy, to_i16(c3.z), to_i16(__fmul_rn(n0, 1000.0f)), t, 0u);
+        const int tx = sm.tm[i].x;
+        const unsigned t = MODE == 0 ? 0u : (unsigned)tx;   // the priority is only read by priority strips
+        const int xy = MODE == 0 ? tx : fb_xy;
+        const int sx = (int)(short)(xy & 0xFFFF), sy = xy >> 16;
+        const float fb_z = sm.fbz[i];
+        emit<MODE>(p, sm, &nent, &sflag, xs0, xs1, sx, sy, to_i16(fb_z), to_i16(__fmul_rn(n0, 1000.0f)), t, 0u);
         if (p.twin) {
-          const float fz2 = __fadd_rn(c3.z, (n0 >= 0.0f) ? -p.shell_off : p.shell_off);
+          const float fz2 = __fadd_rn(fb_z, (n0 >= 0.0f) ? -p.shell_off : p.shell_off);
           emit<MODE>(p, sm, &nent, &sflag, xs0, xs1, sx, sy, to_i16(fz2), to_i16(__fmul_rn(-n0, 1000.0f)), t, 1u);
         }
       }
@@ -1067,8 +1148,15 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 1) k_strip(EngineParams p
     const size_t ob = round16(sizeof(short) * (size_t)HG);
     const size_t cb = strip_chunk_bytes();
     sm.longq = (short*)(chunk + ob);
-    sm.scr = (unsigned*)(chunk + 2 * ob);
-    sm.scr_cap = 2 * ob < cb ? (int)((cb - 2 * ob) / (sizeof(unsigned) * blockDim.x)) : 0;
+    size_t used = 2 * ob;
+    sm.longq2 = nullptr; sm.wbuf = nullptr;
+    if (MODE == 0) {
+      sm.longq2 = (short*)(chunk + 2 * ob);
+      sm.wbuf = (unsigned*)(chunk + 3 * ob);
+      used = 3 * ob + sizeof(unsigned) * kWarpKeys * (blockDim.x >> 5);
+    }
+    sm.scr = (unsigned*)(chunk + used);
+    sm.scr_cap = used < cb ? (int)((cb - used) / (sizeof(unsigned) * blockDim.x)) : 0;
   }
 
   // ---- phase B: column stage over the occupied slots; every occupied
@@ -1097,7 +1185,7 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 1) k_strip(EngineParams p
       d[6] = c.lasttype; d[7] = (p.bed_type != kBedNone) ? bed_flags(p, c) : 0;
     }
   };
-  if (threadIdx.x == 0) nlong = 0;
+  if (threadIdx.x == 0) { nlong = 0; nlong2 = 0; }
   __syncthreads();
   if (!redo) {
     for (int l = threadIdx.x; l < nocc; l += blockDim.x) {
@@ -1118,14 +1206,59 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 1) k_strip(EngineParams p
     }
   }
   __syncthreads();
+  // B2: columns of three or more raw entries, one per thread; in normal
+  // strips those past kRegKeys raw entries go on to B3 instead
   if (!redo) {
     for (int q = threadIdx.x; q < nlong; q += blockDim.x) {
       const int l = sm.longq[q];
       const int ls = sm.olist[l];
+      const int head = sm.heads[ls];
+      bool later = false;
+      if (MODE == 0) {
+        int n = 0;
+        for (int e = head; e >= 0 && n <= kRegKeys; e = sm.enext[e]) n++;
+        later = n > kRegKeys;
+      }
+      const unsigned want = __ballot_sync(__activemask(), later);
+      if (later) {
+        const int lane = threadIdx.x & 31, leader = __ffs(want) - 1;
+        int base = 0;
+        if (lane == leader) base = atomicAdd(&nlong2, __popc(want));
+        base = __shfl_sync(want, base, leader);
+        sm.longq2[base + __popc(want & ((1u << lane) - 1u))] = (short)l;
+        continue;
+      }
       const int gx = xs0 + ls / p.G, gy = ls % p.G;
       const int gslot = gx * p.G + gy;
-      const ColOut c = column<MODE>(p, sm, sm.heads[ls], dump, gslot, &sflag);
+      const ColOut c = column<MODE>(p, sm, head, dump, gslot, &sflag);
       store(l, ls, gx, gy, gslot, c);
+    }
+  }
+  // B3 (normal strips): one warp per column of more than kRegKeys raw entries
+  if (MODE == 0) {
+    __syncthreads();
+    if (!redo) {
+      const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+      unsigned* wbuf = sm.wbuf + wid * kWarpKeys;
+      for (int q = wid; q < nlong2; q += nw) {
+        const int l = sm.longq2[q];
+        const int ls = sm.olist[l];
+        const int head = sm.heads[ls];
+        const int gx = xs0 + ls / p.G, gy = ls % p.G;
+        const int gslot = gx * p.G + gy;
+        int n = 0;
+        if (lane == 0)
+          for (int e = head; e >= 0 && n <= kWarpKeys; e = sm.enext[e]) n++;
+        n = __shfl_sync(0xFFFFFFFFu, n, 0);
+        ColOut c;
+        if (n <= kWarpKeys) {
+          column_warp(p, sm, head, n, wbuf, dump, gslot, &sflag, c);
+        } else if (lane == 0) {
+          c = column<MODE>(p, sm, head, dump, gslot, &sflag);   // a very long list: one thread
+        }
+        if (lane == 0) store(l, ls, gx, gy, gslot, c);
+        __syncwarp();
+      }
     }
   }
 
