@@ -448,6 +448,7 @@ constexpr int kChunk = 256;    // triangles staged per pass (== blockDim.x)
 constexpr int kRegKeys = 8;    // columns with up to this many raw pixels sort in registers
 constexpr int kMaxEnt = 32767; // entry indices are stored as int16
 constexpr int kWarpKeys = 64;  // raw entries a warp sorts in registers (two per lane)
+constexpr int kWalkQueue = 64; // pre-reject survivors queued per warp before the exact test
 
 struct StripSmem {
   int* heads;          // [H*G] first entry of each column list, -1 if empty
@@ -463,6 +464,7 @@ struct StripSmem {
   unsigned* thit;      // [kChunk / 32] triangles with an accepted pixel
   uint8_t* tkind;      // [kChunk] bit 0: fallback only; bit 1: box inside one strip
   float* fbz;          // [kChunk] z of each staged triangle's centroid fallback pixel
+  unsigned* wq;        // [warps][kWalkQueue] pixels past the pre-reject, per warp
   short* olist;        // [H*G] occupied local slots in slot order (aliases the chunk area)
   short* longq;        // [H*G] phase B: positions in olist of columns with three or more raw entries
   short* longq2;       // [H*G] phase B, normal strips: columns of more than kRegKeys raw entries
@@ -474,7 +476,7 @@ struct StripSmem {
 __host__ __device__ inline size_t strip_chunk_bytes()
 {
   return 3 * sizeof(float4) * kChunk + sizeof(int4) * kChunk + sizeof(int) * (kChunk + 4) + sizeof(unsigned) * (kChunk / 32) +
-         sizeof(float) * kChunk + kChunk;
+         sizeof(float) * kChunk + sizeof(unsigned) * kWalkQueue * (kChunk / 32) + kChunk;
 }
 
 __host__ __device__ inline size_t round16(size_t b) { return (b + 15) / 16 * 16; }
@@ -910,6 +912,76 @@ __device__ __forceinline__ void tri_from_smem(const StripSmem& sm, int ti, int x
   r.t = tm.x; r.x0 = tm.y; r.y0 = tm.z; r.ylen = tm.w; r.xc0 = max(tm.y, xlo);
 }
 
+// Triangle constants the pre-reject walk needs (a light TriReg).
+struct TriTest {
+  float ax, ay, e0x, e0y, e1x, e1y, d00, d01, d11;
+  float rlo, rvhi, rwhi, ruhi;   // bounds on the sign-adjusted numerators (ruhi: on their sum)
+  bool dpos;                     // denom > 0
+  int x0, y0, ylen, xc0;
+};
+
+__device__ __forceinline__ void tri_test_from_smem(const StripSmem& sm, int ti, int xlo, TriTest& r)
+{
+  const float4 a4 = sm.q0[ti], b4 = sm.q1[ti], c4 = sm.q2[ti];
+  const int4 tm = sm.tm[ti];
+  TriGeo g;
+  g.ax = a4.x; g.ay = a4.y; g.bx = b4.x; g.by = b4.y; g.cx = c4.x; g.cy = c4.y;
+  Bary b;
+  bary_setup(g, b);
+  r.ax = a4.x; r.ay = a4.y;
+  r.e0x = b.e0x; r.e0y = b.e0y; r.e1x = b.e1x; r.e1y = b.e1y; r.d00 = b.d00; r.d01 = b.d01; r.d11 = b.d11;
+  const float ad = b.denom >= 0.0f ? b.denom : -b.denom;
+  r.dpos = b.denom > 0.0f;
+  r.rlo = __fmul_rn(-0.002f, ad);
+  r.rvhi = __fmul_rn(1.002f, ad);
+  r.rwhi = __fmul_rn(1.004f, ad);
+  r.ruhi = __fmul_rn(1.003f, ad);
+  r.x0 = tm.y; r.y0 = tm.z; r.ylen = tm.w; r.xc0 = max(tm.y, xlo);
+}
+
+// The exact test and emission of one queued pixel: item = triangle index in
+// the chunk << 24 | column offset from the first walked column << 12 | row
+// offset from the box's first row.  _getBaryCoord (Tomo_types.cpp:86-115)
+// in the reference's operation order, u formed in double; an accepted pixel
+// is interpolated (_bary_product, Tomo_types.cpp:75-84) and appended with its
+// shell twin (triVoxel, STomoSh_INT3.cpp:1160-1188), and its triangle is
+// marked as hit for the centroid fallback.
+template <int MODE>
+__device__ __forceinline__ void exact_item(const EngineParams& p, const StripSmem& sm, int* nent, int* sflag, int xs0,
+                                           int xs1, int xlo, unsigned item, float half, float vmax)
+{
+  const int ti = (int)(item >> 24);
+  TriReg r;
+  tri_from_smem(sm, ti, xlo, r);
+  const int x = r.xc0 + (int)((item >> 12) & 0xFFFu), y = r.y0 + (int)(item & 0xFFFu);
+  const float px = pix_center(x, half);
+  const float ex0 = __fmul_rn(__fsub_rn(px, r.ax), r.b.e0x);
+  const float ex1 = __fmul_rn(__fsub_rn(px, r.ax), r.b.e1x);
+  const float e2y = __fsub_rn(pix_center(y, half), r.ay);
+  const float d20 = __fadd_rn(ex0, __fmul_rn(e2y, r.b.e0y));
+  const float d21 = __fadd_rn(ex1, __fmul_rn(e2y, r.b.e1y));
+  const float vn = __fsub_rn(__fmul_rn(r.b.d11, d20), __fmul_rn(r.b.d01, d21));
+  const float wn = __fsub_rn(__fmul_rn(r.b.d00, d21), __fmul_rn(r.b.d01, d20));
+  const float v = __fdiv_rn(vn, r.b.denom);
+  const float w = __fdiv_rn(wn, r.b.denom);
+  const float u = __double2float_rn(__dsub_rn(__dsub_rn(1.0, (double)v), (double)w));
+  if (!((u >= -0.001f) && (v >= -0.001f) && (v <= vmax) && (__fadd_rn(u, v) <= vmax))) return;
+  atomicOr(&sm.thit[ti >> 5], 1u << (ti & 31));
+  const float fx = bary3(r.ax, r.bx, r.cx, u, v, w);
+  const float fy = bary3(r.ay, r.by, r.cy, u, v, w);
+  const float fz = bary3(r.az, r.bz, r.cz, u, v, w);
+  const float fn = bary3(r.n0, r.n1, r.n2, u, v, w);
+  const int sx = __float2int_rz(fx), sy = __float2int_rz(fy);
+  const unsigned lidx = (unsigned)((x - r.x0) * r.ylen + (y - r.y0));
+  emit<MODE>(p, sm, nent, sflag, xs0, xs1, sx, sy, to_i16(fz), to_i16(__fmul_rn(fn, 1000.0f)), (unsigned)r.t,
+             lidx * 2u);
+  if (p.twin) {
+    const float fz2 = __fadd_rn(fz, (fn >= 0.0f) ? -p.shell_off : p.shell_off);
+    emit<MODE>(p, sm, nent, sflag, xs0, xs1, sx, sy, to_i16(fz2), to_i16(__fmul_rn(-fn, 1000.0f)), (unsigned)r.t,
+               lidx * 2u + 1u);
+  }
+}
+
 template <int MODE>
 __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 1) k_strip(EngineParams p)
 {
@@ -946,6 +1018,7 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 1) k_strip(EngineParams p
   sm.pref = (int*)q; q += sizeof(int) * (kChunk + 4);
   sm.thit = (unsigned*)q; q += sizeof(unsigned) * (kChunk / 32);
   sm.fbz = (float*)q; q += sizeof(float) * kChunk;
+  sm.wq = (unsigned*)q; q += sizeof(unsigned) * kWalkQueue * (kChunk / 32);
   sm.tkind = (uint8_t*)q; q += kChunk;
   sm.olist = (short*)chunk;
 
@@ -1020,84 +1093,89 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 1) k_strip(EngineParams p
     if (i == 0) sm.pref[kChunk] = total;
     __syncthreads();
 
-    // each thread walks a contiguous range of (triangle, pixel) items
-    const int per = (total + blockDim.x - 1) / blockDim.x;
+    // Each thread walks a contiguous range of (triangle, pixel) items with
+    // the pre-reject test only; the pixels it lets through are queued per
+    // warp (shared memory, 64 slots) and, 32 at a time, every lane of the
+    // warp runs the exact barycentric test and the pixel's emission on one
+    // of them -- so the divisions, the double-precision u and the append run
+    // on full warps instead of on the few lanes whose item passed.
+    const int per = (total + blockDim.x - 1) / blockDim.x;   // CTA-uniform trip count
     const int j0 = min(i * per, total), j1 = min(j0 + per, total);
+    const int lane = i & 31;
+    unsigned* wq = sm.wq + (i >> 5) * kWalkQueue;
+    int qn = 0;   // warp-uniform queue length
+    TriTest r;
+    int ti = 0, x = 0, y = 0, yend = 0, tnext = 0;
+    float ex0 = 0.f, ex1 = 0.f;
     if (j0 < j1) {
       int lo = 0, hi = nchunk - 1;
       while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
         if (sm.pref[mid] <= j0) lo = mid; else hi = mid - 1;
       }
-      int ti = lo;
-      TriReg r;
-      tri_from_smem(sm, ti, xlo, r);
+      ti = lo;
+      tri_test_from_smem(sm, ti, xlo, r);
       const int k = j0 - sm.pref[ti];
-      int x = r.xc0 + k / r.ylen;
-      int y = r.y0 + k % r.ylen;
-      int yend = r.y0 + r.ylen - 1;
-      int tnext = sm.pref[ti + 1];
-      // Per pixel this is _getBaryCoord (Tomo_types.cpp:86-115) with the
-      // x-only products hoisted per column and the "+ 0*0" terms of _dot left
-      // out (they can only turn -0 into +0, which changes no comparison and no
-      // stored value).  A pixel whose sign-adjusted numerators lie clearly
-      // outside the acceptance box -- by twice the 0.001 margin -- is rejected
-      // before the divisions; every such pixel fails the exact test too.
-      float px = pix_center(x, half);
-      float ex0 = __fmul_rn(__fsub_rn(px, r.ax), r.b.e0x);
-      float ex1 = __fmul_rn(__fsub_rn(px, r.ax), r.b.e1x);
-      bool hit_any = false;
-      for (int j = j0; j < j1; j++) {
+      x = r.xc0 + k / r.ylen;
+      y = r.y0 + k % r.ylen;
+      yend = r.y0 + r.ylen - 1;
+      tnext = sm.pref[ti + 1];
+      const float px = pix_center(x, half);
+      ex0 = __fmul_rn(__fsub_rn(px, r.ax), r.e0x);
+      ex1 = __fmul_rn(__fsub_rn(px, r.ax), r.e1x);
+    }
+    for (int it = 0; it < per; it++) {
+      const int j = j0 + it;
+      bool pass = false;
+      unsigned item = 0u;
+      if (j < j1) {
+        // The pre-reject: _getBaryCoord's numerators (Tomo_types.cpp:86-115) with
+        // the x-only products hoisted per column and the "+ 0*0" terms of _dot
+        // left out (they can only turn -0 into +0, which changes no comparison
+        // and no stored value); a pixel whose sign-adjusted numerators lie
+        // outside the acceptance region by twice the 0.001 margin -- v or w out
+        // of range, or v + w past 1 -- fails the exact test too.
         const float e2y = __fsub_rn(pix_center(y, half), r.ay);
-        const float d20 = __fadd_rn(ex0, __fmul_rn(e2y, r.b.e0y));
-        const float d21 = __fadd_rn(ex1, __fmul_rn(e2y, r.b.e1y));
-        const float vn = __fsub_rn(__fmul_rn(r.b.d11, d20), __fmul_rn(r.b.d01, d21));
-        const float wn = __fsub_rn(__fmul_rn(r.b.d00, d21), __fmul_rn(r.b.d01, d20));
+        const float d20 = __fadd_rn(ex0, __fmul_rn(e2y, r.e0y));
+        const float d21 = __fadd_rn(ex1, __fmul_rn(e2y, r.e1y));
+        const float vn = __fsub_rn(__fmul_rn(r.d11, d20), __fmul_rn(r.d01, d21));
+        const float wn = __fsub_rn(__fmul_rn(r.d00, d21), __fmul_rn(r.d01, d20));
         const float vs = r.dpos ? vn : -vn, ws = r.dpos ? wn : -wn;
-        if (!(vs < r.rlo || vs > r.rvhi || ws < r.rlo || ws > r.rwhi)) {
-          const float v = __fdiv_rn(vn, r.b.denom);
-          const float w = __fdiv_rn(wn, r.b.denom);
-          const float u = __double2float_rn(__dsub_rn(__dsub_rn(1.0, (double)v), (double)w));
-          if ((u >= -0.001f) && (v >= -0.001f) && (v <= vmax) && (__fadd_rn(u, v) <= vmax)) {
-            hit_any = true;
-            const float fx = bary3(r.ax, r.bx, r.cx, u, v, w);
-            const float fy = bary3(r.ay, r.by, r.cy, u, v, w);
-            const float fz = bary3(r.az, r.bz, r.cz, u, v, w);
-            const float fn = bary3(r.n0, r.n1, r.n2, u, v, w);
-            const int sx = __float2int_rz(fx), sy = __float2int_rz(fy);
-            const unsigned lidx = (unsigned)((x - r.x0) * r.ylen + (y - r.y0));
-            emit<MODE>(p, sm, &nent, &sflag, xs0, xs1, sx, sy, to_i16(fz), to_i16(__fmul_rn(fn, 1000.0f)),
-                       (unsigned)r.t, lidx * 2u);
-            if (p.twin) {
-              const float fz2 = __fadd_rn(fz, (fn >= 0.0f) ? -p.shell_off : p.shell_off);
-              emit<MODE>(p, sm, &nent, &sflag, xs0, xs1, sx, sy, to_i16(fz2), to_i16(__fmul_rn(-fn, 1000.0f)),
-                         (unsigned)r.t, lidx * 2u + 1u);
-            }
-          }
-        }
+        pass = !(vs < r.rlo || vs > r.rvhi || ws < r.rlo || ws > r.rwhi || __fadd_rn(vs, ws) > r.ruhi);
+        item = ((unsigned)ti << 24) | ((unsigned)(x - r.xc0) << 12) | (unsigned)(y - r.y0);
         // advance to item j + 1
         if (j + 1 == tnext) {
-          if (hit_any) atomicOr(&sm.thit[ti >> 5], 1u << (ti & 31));
-          hit_any = false;
           if (j + 1 < j1) {
             ti++;
             while (sm.pref[ti + 1] <= j + 1) ti++;   // skip triangles without pixels here
-            tri_from_smem(sm, ti, xlo, r);
+            tri_test_from_smem(sm, ti, xlo, r);
             x = r.xc0; y = r.y0; yend = r.y0 + r.ylen - 1;
             tnext = sm.pref[ti + 1];
-            px = pix_center(x, half);
-            ex0 = __fmul_rn(__fsub_rn(px, r.ax), r.b.e0x);
-            ex1 = __fmul_rn(__fsub_rn(px, r.ax), r.b.e1x);
+            const float px = pix_center(x, half);
+            ex0 = __fmul_rn(__fsub_rn(px, r.ax), r.e0x);
+            ex1 = __fmul_rn(__fsub_rn(px, r.ax), r.e1x);
           }
         } else if (++y > yend) {
           y = r.y0; x++;
-          px = pix_center(x, half);
-          ex0 = __fmul_rn(__fsub_rn(px, r.ax), r.b.e0x);
-          ex1 = __fmul_rn(__fsub_rn(px, r.ax), r.b.e1x);
+          const float px = pix_center(x, half);
+          ex0 = __fmul_rn(__fsub_rn(px, r.ax), r.e0x);
+          ex1 = __fmul_rn(__fsub_rn(px, r.ax), r.e1x);
         }
       }
-      if (hit_any) atomicOr(&sm.thit[ti >> 5], 1u << (ti & 31));
+      const unsigned m = __ballot_sync(0xFFFFFFFFu, pass);
+      if (pass) wq[qn + __popc(m & ((1u << lane) - 1u))] = item;
+      qn += __popc(m);
+      if (qn >= 32) {
+        __syncwarp();
+        exact_item<MODE>(p, sm, &nent, &sflag, xs0, xs1, xlo, wq[lane], half, vmax);
+        __syncwarp();
+        if (lane < qn - 32) wq[lane] = wq[lane + 32];
+        qn -= 32;
+        __syncwarp();
+      }
     }
+    __syncwarp();
+    if (lane < qn) exact_item<MODE>(p, sm, &nent, &sflag, xs0, xs1, xlo, wq[lane], half, vmax);
     __syncthreads();
     // centroid fallback of triangles without any accepted pixel
     if (i < nchunk) {
