@@ -158,13 +158,23 @@ __device__ __forceinline__ float centroid(float a, float b, float c)
 // Whether any pixel centre of the box passes the barycentric test.  Pixels
 // whose sign-adjusted numerators lie outside the acceptance box by twice the
 // 0.001 margin are rejected before the divisions (the same pre-reject as the
-// strip walk; every such pixel fails the exact test too).
+// strip walk; every such pixel fails the exact test too).  The pixel nearest
+// the centroid is tried first: for all but the smallest triangles it is
+// inside, and the box scan is skipped.
 __device__ bool any_hit(const EngineParams& p, const TriGeo& g, const Bary& b)
 {
   if (!b.ok) return false;
   const float ad = b.denom >= 0.0f ? b.denom : -b.denom;
   const bool dpos = b.denom > 0.0f;
   const float rlo = __fmul_rn(-0.002f, ad), rvhi = __fmul_rn(1.002f, ad), rwhi = __fmul_rn(1.004f, ad);
+  {
+    // a guess only (any pixel of the box would do), so its rounding does not matter
+    const float mx = (g.ax + g.bx + g.cx) * (1.0f / 3.0f), my = (g.ay + g.by + g.cy) * (1.0f / 3.0f);
+    const int x = min(max(__float2int_rd(mx - p.half), g.x0), g.x1);
+    const int y = min(max(__float2int_rd(my - p.half), g.y0), g.y1);
+    float u, v, w;
+    if (bary_test(g.ax, g.ay, b, pix_center(x, p.half), pix_center(y, p.half), p.vmax, u, v, w)) return true;
+  }
   for (int x = g.x0; x <= g.x1; x++) {
     const float px = pix_center(x, p.half);
     const float e2x = __fsub_rn(px, g.ax);
