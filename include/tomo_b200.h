@@ -93,7 +93,8 @@ void tomoVolToMass(const float* f32info, const int* i32info, float* vm22);
 #define TOMO_OPT_EXPORT 5       /* 0 = skip the best orientation's pixel export (default 1) */
 #define TOMO_OPT_ADAPTIVE 6     /* 0 = keep the planned strip budget even when early batches overflow (default 1) */
 #define TOMO_OPT_PROPOSAL 7     /* tomoSurrogateSearch proposals: 0 = the trained network (default), 1 = bilinear
-                                   interpolation of the exact coarse values (the search without the network) */
+                                   interpolation of the exact coarse values (the search without the network),
+                                   2 = the mean of the two */
 int tomoSetOption(int key, int value);
 
 /* out[0..8] = grid edge, strip height, strips, entry capacity, orientations re-run

@@ -191,7 +191,8 @@ constexpr int kMaxGrid = 4096;
 int g_static_reruns[5];
 
 // Proposal source of tomoSurrogateSearch: 0 the trained network, 1 bilinear
-// interpolation of the exact coarse values (the search without the network).
+// interpolation of the exact coarse values (the search without the network),
+// 2 the mean of the two.
 int g_proposal = 0;
 
 struct BatchSet {   // per-batch buffers read by the fold, double-buffered
@@ -1392,7 +1393,7 @@ int tomoSetOption(int key, int value)
     case TOMO_OPT_NORMAL_SMEM: if (value < 0 || value > 232448) return TOMO_ERR_ARG; E.normal_smem = value; return 0;
     case TOMO_OPT_EXPORT: E.export_pixels = value ? 1 : 0; return 0;
     case TOMO_OPT_ADAPTIVE: E.adaptive = value ? 1 : 0; E.adapt_smem = E.adapt_h = E.adapt_cfg = 0; return 0;
-    case TOMO_OPT_PROPOSAL: if (value < 0 || value > 1) return TOMO_ERR_ARG; g_proposal = value; return 0;
+    case TOMO_OPT_PROPOSAL: if (value < 0 || value > 2) return TOMO_ERR_ARG; g_proposal = value; return 0;
     default: return TOMO_ERR_ARG;
   }
 }
@@ -2395,12 +2396,9 @@ int tomoSurrogateSearch(const float* f32info, const int* i32info, const float* Y
       for (int iy = 0; iy < n_yaw; iy += stride) coarse.push_back(ip * n_yaw + iy);
     n_coarse = (int)coarse.size();
     TOMO_TRY(evaluate(coarse));
-    if (g_proposal == 1) {
-      // 2'-3'. the search without the network: the exact coarse Vss,
-      // bilinearly interpolated onto every grid point (yaw wraps around);
-      // the coarse points are exact, so the error is measured on the
-      // refined points only
-      const auto t0 = std::chrono::steady_clock::now();
+    // bilinear interpolation of the exact coarse Vss onto every grid point
+    // (yaw wraps around): the proposal of the search without the network
+    auto interpolate = [&](std::vector<float>& out) {
       const int ncyc = (n_yaw + stride - 1) / stride, ncpc = (n_pitch + stride - 1) / stride;
       auto cval = [&](int p, int y) { return (double)E.vss64[(size_t)(p * stride) * n_yaw + (size_t)(y * stride)]; };
       for (int ip = 0; ip < n_pitch; ip++) {
@@ -2413,9 +2411,15 @@ int tomoSurrogateSearch(const float* f32info, const int* i32info, const float* Y
           const double wy = fy - std::floor(fy);
           const double r0 = cval(p0, y0) * (1.0 - wy) + cval(p0, y1) * wy;
           const double r1 = cval(p1, y0) * (1.0 - wy) + cval(p1, y1) * wy;
-          pred[(size_t)ip * n_yaw + iy] = (float)((1.0 - wp) * r0 + wp * r1);
+          out[(size_t)ip * n_yaw + iy] = (float)((1.0 - wp) * r0 + wp * r1);
         }
       }
+    };
+    if (g_proposal == 1) {
+      // 2'-3'. the search without the network; the coarse points are exact,
+      // so the error is measured on the refined points only
+      const auto t0 = std::chrono::steady_clock::now();
+      interpolate(pred);
       for (int id : coarse) trained[id] = 1;
       t_pred += seconds_since(t0);
     } else {
@@ -2477,6 +2481,11 @@ int tomoSurrogateSearch(const float* f32info, const int* i32info, const float* Y
         TOMO_CUDA(cudaMemcpyAsync(pred.data(), dy.ptr, sizeof(float) * n, cudaMemcpyDeviceToHost, E.main));
         TOMO_CUDA(cudaStreamSynchronize(E.main));
         for (int id = 0; id < n; id++) pred[id] = (float)inv(pred[id] * sd + mean);
+        if (g_proposal == 2) {   // the network and the interpolation, averaged
+          std::vector<float> lin(n);
+          interpolate(lin);
+          for (int id = 0; id < n; id++) pred[id] = 0.5f * (pred[id] + lin[id]);
+        }
         t_pred += seconds_since(t0);
       }
       dypr.release();

@@ -99,11 +99,14 @@ def search(mesh, ypr, n_yaw: int, n_pitch: int, opts, stride: int = 10, cell: in
 
     ``proposal="interpolation"`` runs the same search without the network:
     the blocks are ranked by a bilinear interpolation of the exact coarse
-    values and the error gate uses that interpolation's observed error."""
+    values and the error gate uses that interpolation's observed error;
+    ``proposal="mean"`` ranks by the mean of the network and that
+    interpolation."""
     from .native import TOMO_OPT_PROPOSAL
     from .options import pack_info
-    if proposal not in ("network", "interpolation"):
-        raise ValueError("proposal must be 'network' or 'interpolation'")
+    modes = {"network": 0, "interpolation": 1, "mean": 2}
+    if proposal not in modes:
+        raise ValueError("proposal must be 'network', 'interpolation' or 'mean'")
     f32, i32 = pack_info(opts, mesh, ypr.shape[0])
     ypr, tri, vtx, vn, *_ = _arrays(mesh, ypr)
     n = ypr.shape[0]
@@ -114,7 +117,7 @@ def search(mesh, ypr, n_yaw: int, n_pitch: int, opts, stride: int = 10, cell: in
     mss = np.zeros(n, np.float32)
     pred = np.zeros(n, np.float32)
     st = np.zeros(12, np.float64)
-    _check(_lib().tomoSetOption(TOMO_OPT_PROPOSAL, 1 if proposal == "interpolation" else 0))
+    _check(_lib().tomoSetOption(TOMO_OPT_PROPOSAL, modes[proposal]))
     try:
         opt = _check(_lib().tomoSurrogateSearch(_p(f32, _f32p), _p(i32, _i32p), _p(ypr, _f32p), _p(tri, _i32p),
                                                 _p(vtx, _f32p), _p(vn, _f32p), int(n_yaw), int(n_pitch),
