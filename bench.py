@@ -134,7 +134,7 @@ class ClockSampler:
 # ------------------------------------------------------------------ CPU baseline
 
 def cpu_baseline(mesh, ypr, opts, grid, budget_s: float, gpu_vss=None, threads: int | None = None,
-                 n: int | None = None):
+                 n: int | None = None, gpu_mss=None):
     """The reference INT3 engine (oracle/_ref, built from the reference sources)
     -- or, if that library is absent, the oracle's C restatement -- on an
     evenly strided sample of the workload's orientations, all host threads."""
@@ -175,6 +175,9 @@ def cpu_baseline(mesh, ypr, opts, grid, budget_s: float, gpu_vss=None, threads: 
            "sample": f"{n} of the {n_all} orientations, evenly strided, one call, {dt:.1f} s"}
     if gpu_vss is not None and "Vss64" in out:
         res["sample_vss_bit_identical"] = bool(np.array_equal(out["Vss64"], gpu_vss[idx]))
+    if gpu_mss is not None and "Mss" in out:
+        res["sample_mss_bit_identical"] = bool(np.array_equal(np.asarray(out["Mss"], np.float32).view(np.int32),
+                                                              np.asarray(gpu_mss, np.float32)[idx].view(np.int32)))
     return res
 
 
@@ -339,7 +342,7 @@ def run_ours(args, rank, world, local_rank):
             "clocks": clk.summary()}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(mesh, ypr, opts, grid, budget_s=args.cpu_budget_s,
-                                            gpu_vss=res["Vss64"])
+                                            gpu_vss=res["Vss64"], gpu_mss=Mss)
         # the same engine on one host thread, on a smaller sample
         one = cpu_baseline(mesh, ypr, opts, grid, budget_s=args.cpu_budget_s / 2, gpu_vss=res["Vss64"], threads=1)
         line["cpu_baseline"]["single_thread"] = {k: one[k] for k in ("value", "unit", "cores", "kind", "sample")
@@ -441,7 +444,7 @@ def main():
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the plain-launch, batched and surrogate figures added to the line")
     ap.add_argument("--batched-meshes", type=int, default=16)
-    ap.add_argument("--surrogate-meshes", type=int, default=10)
+    ap.add_argument("--surrogate-meshes", type=int, default=100)
     ap.add_argument("--suite", choices=("none", "batched", "surrogate", "shell"), default="none",
                     help="run a full-size suite instead (64 uneven meshes / 100 searched meshes)")
     ap.add_argument("--max-orientations", type=int, default=0,

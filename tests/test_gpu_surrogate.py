@@ -95,3 +95,27 @@ def test_bed_falls_back_to_exhaustive():
     r = surrogate.search(mesh, ypr, 36, 7, opts, stride=2, cell=2)
     assert r.fallback and r.evaluated == ypr.shape[0]
     assert r.optID == ex.optID and np.array_equal(r.Mss.view(np.int32), ex.Mss.view(np.int32))
+
+
+@pytest.mark.parametrize("seed", [31, 32, 33])
+def test_search_with_and_without_the_network(seed):
+    """The ablation: the same coarse-to-fine search with blocks ranked by the
+    trained network, by a bilinear interpolation of the exact coarse values
+    (no network), and by the mean of the two.  Each must reach the exhaustive
+    sweep's optimal Mss with exact values wherever it evaluated, while
+    evaluating a small fraction of the grid; the evaluation counts of the
+    three are printed side by side (the suite in bench.py reports them over
+    100 meshes)."""
+    mesh = meshgen.small_solid(seed, with_hull=False)
+    ypr = meshgen.ypr_grid(np.arange(0, 360, 0.5), np.arange(0, 60.5, 0.5))
+    opts = PrintOptions(explicit_ss=True)
+    ex = native.sweep(mesh, ypr, opts)
+    counts = {}
+    for kind in ("network", "interpolation", "mean"):
+        r = surrogate.search(mesh, ypr, 720, 121, opts, seed=seed, proposal=kind)
+        assert np.float32(r.Mss[r.optID]) == ex.Mss[ex.optID], f"{kind}: optimum value differs from the exhaustive sweep"
+        done = ~np.isnan(r.Mss)
+        assert np.array_equal(r.Mss[done].view(np.int32), ex.Mss[done].view(np.int32)), f"{kind}: evaluated Mss not exact"
+        assert r.evaluated < 0.1 * ypr.shape[0], f"{kind}: evaluated {r.evaluated} of {ypr.shape[0]}"
+        counts[kind] = (r.evaluated, round(r.seconds * 1e3, 1), round(r.max_abs_error, 1))
+    print(f"seed {seed}: (evaluated, ms, max abs error) {counts}")
