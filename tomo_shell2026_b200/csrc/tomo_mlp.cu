@@ -389,6 +389,7 @@ Mlp::~Mlp() { free_all(); }
 
 void Mlp::free_all()
 {
+  if (fit_exec_) { cudaGraphExecDestroy(fit_exec_); fit_exec_ = nullptr; }
   for (float** p : {&params_, &wt_, &grads_, &m_, &v_, &x_, &y_, &loss_, &part_, &part_loss_})
     if (*p) { cudaFree(*p); *p = nullptr; }
   cap_ = 0; n_ = 0; steps_done_ = 0;
@@ -513,7 +514,31 @@ cudaError_t Mlp::adam(float lr, cudaStream_t s)
 cudaError_t Mlp::fit(int steps, float lr, cudaStream_t s, float* final_loss)
 {
   if (n_ <= 0 || steps < 0) return cudaErrorInvalidValue;
-  for (int i = 0; i < steps; i++) MLP_TRY(step(lr, true, s));
+  if (steps > 0) {
+    // Adam's bias corrections are launch arguments, so a graph is tied to
+    // the step it starts from as well as to the shapes and buffers
+    const bool reuse = fit_exec_ && fit_n_ == n_ && fit_steps_ == steps && fit_lr_ == lr &&
+                       fit_start_ == steps_done_ && fit_bufs_[0] == x_ && fit_bufs_[1] == y_ && fit_bufs_[2] == part_;
+    if (!reuse) {
+      if (fit_exec_) { cudaGraphExecDestroy(fit_exec_); fit_exec_ = nullptr; }
+      MLP_TRY(configure());
+      const int start = steps_done_;
+      MLP_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+      cudaError_t e = cudaSuccess;
+      for (int i = 0; i < steps && e == cudaSuccess; i++) e = step(lr, true, s);
+      cudaGraph_t g = nullptr;
+      const cudaError_t e2 = cudaStreamEndCapture(s, &g);
+      steps_done_ = start;
+      if (e == cudaSuccess) e = e2;
+      if (e == cudaSuccess) e = cudaGraphInstantiate(&fit_exec_, g, 0);
+      if (g) cudaGraphDestroy(g);
+      if (e != cudaSuccess) { fit_exec_ = nullptr; return e; }
+      fit_n_ = n_; fit_steps_ = steps; fit_lr_ = lr; fit_start_ = start;
+      fit_bufs_[0] = x_; fit_bufs_[1] = y_; fit_bufs_[2] = part_;
+    }
+    MLP_TRY(cudaGraphLaunch(fit_exec_, s));
+    steps_done_ += steps;
+  }
   if (final_loss) {
     MLP_TRY(cudaMemcpyAsync(final_loss, loss_, sizeof(float), cudaMemcpyDeviceToHost, s));
     MLP_TRY(cudaStreamSynchronize(s));

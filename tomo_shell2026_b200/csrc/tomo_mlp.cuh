@@ -48,7 +48,9 @@ class Mlp {
   cudaError_t read_grad(float* host, float* loss, cudaStream_t s);
   // One Adam step from the current gradient.
   cudaError_t adam(float lr, cudaStream_t s);
-  // steps x (grad + Adam).
+  // steps x (grad + Adam), replayed as one captured CUDA graph: the graph of a
+  // (sample count, steps, learning rate, starting step, buffers) combination
+  // is kept and replayed by later fits with the same combination.
   cudaError_t fit(int steps, float lr, cudaStream_t s, float* final_loss);
   // Prediction for n device feature rows.
   cudaError_t predict_device(const float* dev_x, int n, float* dev_out, cudaStream_t s);
@@ -65,6 +67,10 @@ class Mlp {
   float *x_ = nullptr, *y_ = nullptr, *loss_ = nullptr;
   float *part_ = nullptr, *part_loss_ = nullptr;   // per-block gradients [blocks][total], losses [blocks]
   int cap_ = 0, n_ = 0, steps_done_ = 0;
+  cudaGraphExec_t fit_exec_ = nullptr;     // the last captured fit and what it was captured for
+  int fit_n_ = 0, fit_steps_ = 0, fit_start_ = -1;
+  float fit_lr_ = 0.f;
+  const float* fit_bufs_[3] = {nullptr, nullptr, nullptr};
 };
 
 }  // namespace tomo
