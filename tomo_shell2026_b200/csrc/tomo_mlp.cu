@@ -27,7 +27,7 @@ namespace tomo {
 
 namespace {
 
-constexpr int kSB = 16;          // samples per CTA
+constexpr int kSB = 8;           // samples per CTA
 constexpr int kQ = kSB / 2;      // samples per thread (two groups of 128 threads)
 constexpr int kThreads = 256;
 constexpr int kH = kMlpHidden;   // 128
