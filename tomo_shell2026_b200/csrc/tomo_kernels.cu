@@ -1010,7 +1010,13 @@ __device__ __forceinline__ void exact_item(const EngineParams& p, const StripSme
   const float w = __fdiv_rn(wn, r.b.denom);
   const float u = __double2float_rn(__dsub_rn(__dsub_rn(1.0, (double)v), (double)w));
   if (!((u >= -0.001f) && (v >= -0.001f) && (v <= vmax) && (__fadd_rn(u, v) <= vmax))) return;
-  atomicOr(&sm.thit[ti >> 5], 1u << (ti & 31));
+  {
+    // mark the triangle as hit: one shared atomic per distinct word among the
+    // warp's hitting lanes (they mostly share a few triangles)
+    const unsigned peers = __match_any_sync(__activemask(), ti >> 5);
+    const unsigned bits = __reduce_or_sync(peers, 1u << (ti & 31));
+    if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicOr(&sm.thit[ti >> 5], bits);
+  }
   const float fx = bary3(r.ax, r.bx, r.cx, u, v, w);
   const float fy = bary3(r.ay, r.by, r.cy, u, v, w);
   const float fz = bary3(r.az, r.bz, r.cz, u, v, w);
