@@ -22,7 +22,6 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
-#include <memory>
 #include <map>
 #include <mutex>
 #include <string>
@@ -1899,14 +1898,7 @@ namespace tomo {
 namespace {
 
 struct MultiEngine {
-  // Meshes are spread over up to kLanes workspaces (streams and batch
-  // buffers each), balanced by estimated cost; the captured graph forks from
-  // the first workspace's main stream into the others and joins back, so
-  // small meshes' kernels overlap instead of queueing behind one another.
-  static constexpr int kLanes = 4;
-  std::vector<std::unique_ptr<Workspace>> ws;
-  Workspace& W0() { return *ws[0]; }
-  std::vector<cudaEvent_t> fork_join;   // [0] fork, [1..] joins
+  Workspace W;
   std::vector<Engine*> meshes;
   std::vector<int> order;   // capture order: estimated cost, largest first
   std::map<std::pair<int, int>, Engine::TuneResult> tuned;
@@ -1933,74 +1925,18 @@ struct MultiEngine {
     for (auto* e : meshes) { e->release(); delete e; }
     meshes.clear(); order.clear(); choice.clear();
   }
-  void release()
-  {
-    clear_graph();
-    clear_meshes();
-    for (cudaEvent_t e : fork_join) cudaEventDestroy(e);
-    fork_join.clear();
-    for (auto& w : ws) w->release();
-    ws.clear();
-    tuned.clear();
-  }
-
-  // Records the fork on the first workspace's main stream and makes every
-  // other workspace's main stream wait for it (inside a capture this joins
-  // them to the graph).
-  int fork()
-  {
-    TOMO_CUDA(cudaEventRecord(fork_join[0], W0().main));
-    for (size_t k = 1; k < ws.size(); k++) TOMO_CUDA(cudaStreamWaitEvent(ws[k]->main, fork_join[0], 0));
-    return 0;
-  }
-  int join()
-  {
-    for (size_t k = 1; k < ws.size(); k++) {
-      TOMO_CUDA(cudaEventRecord(fork_join[k], ws[k]->main));
-      TOMO_CUDA(cudaStreamWaitEvent(W0().main, fork_join[k], 0));
-    }
-    return 0;
-  }
-  long long launches() const
-  {
-    long long c = 0;
-    for (const auto& w : ws)
-      for (long long x : w->log.launches) c += x;
-    return c;
-  }
+  void release() { clear_graph(); clear_meshes(); W.release(); tuned.clear(); }
 
   int prepare(int n, const float* const* f32, const int* const* i32, const float* const* ypr, const int* const* tri,
               const float* const* vtx, const float* const* vnrm)
   {
     clear_graph();
     clear_meshes();
-    if (f32 == nullptr || i32 == nullptr) return set_error(TOMO_ERR_ARG, "info arrays are null");
-    for (int m = 0; m < n; m++)
-      if (f32[m] == nullptr || i32[m] == nullptr)
-        return set_error(TOMO_ERR_ARG, "mesh " + std::to_string(m) + ": info arrays are null");
-    // workspaces, and each mesh's by greedy balancing of orientations x triangles
-    const int lanes = std::max(1, std::min(kLanes, n));
-    while ((int)ws.size() < lanes) ws.emplace_back(new Workspace());
-    for (auto& w : ws) TOMO_TRY(w->init());
-    while (fork_join.size() < ws.size()) {
-      cudaEvent_t e = nullptr;
-      TOMO_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-      fork_join.push_back(e);
-    }
-    std::vector<int> lane_of(n, 0), by_cost(n);
-    {
-      std::vector<double> load(ws.size(), 0.0);
-      auto est = [&](int m) { return (double)std::max(i32[m][6], 0) * ((double)std::max(i32[m][4], 0) + 4096.0); };
-      for (int m = 0; m < n; m++) by_cost[m] = m;
-      std::stable_sort(by_cost.begin(), by_cost.end(), [&](int a, int b) { return est(a) > est(b); });
-      for (int m : by_cost) {
-        const int k = (int)(std::min_element(load.begin(), load.end()) - load.begin());
-        lane_of[m] = k;
-        load[k] += est(m);
-      }
-    }
+    TOMO_TRY(W.init());
     for (int m = 0; m < n; m++) {
-      Engine* e = new Engine(*ws[lane_of[m]]);
+      if (f32 == nullptr || i32 == nullptr || f32[m] == nullptr || i32[m] == nullptr)
+        return set_error(TOMO_ERR_ARG, "mesh " + std::to_string(m) + ": info arrays are null");
+      Engine* e = new Engine(W);
       e->adaptive = 0;   // captured into a graph: no host waits inside the sweep
       meshes.push_back(e);
       const int rc = e->upload(f32[m], i32[m], ypr ? ypr[m] : nullptr, tri ? tri[m] : nullptr, vtx ? vtx[m] : nullptr,
@@ -2049,12 +1985,11 @@ struct MultiEngine {
   std::vector<const void*> buffer_addresses() const
   {
     std::vector<const void*> v;
-    for (const auto& w : ws) {
-      for (const auto& q : w->prep)
-        v.insert(v.end(), {q.xf.ptr, q.minkey.ptr, q.trange.ptr, q.bin_off.ptr, q.bin_cur.ptr, q.bins.ptr,
-                           q.bbox.ptr, q.bedf.ptr});
-      for (const auto& st : w->set)
-        v.insert(v.end(), {st.acc.ptr, st.flags.ptr, st.foldcnt.ptr, st.foldv.ptr, st.foldtc.ptr, st.foldmeta.ptr});
+    for (const auto& q : W.prep)
+      v.insert(v.end(), {q.xf.ptr, q.minkey.ptr, q.trange.ptr, q.bin_off.ptr, q.bin_cur.ptr, q.bins.ptr, q.bbox.ptr,
+                         q.bedf.ptr});
+    for (const auto& st : W.set) {
+      v.insert(v.end(), {st.acc.ptr, st.flags.ptr, st.foldcnt.ptr, st.foldv.ptr, st.foldtc.ptr, st.foldmeta.ptr});
     }
     for (const Engine* e : meshes) {
       v.insert(v.end(), {e->vpos.ptr, e->vnrm.ptr, e->tri.ptr, e->rot.ptr, e->ori.ptr, e->o_vo.ptr, e->o_vss.ptr,
@@ -2080,18 +2015,20 @@ struct MultiEngine {
   int capture()
   {
     clear_graph();
-    std::vector<char> timing(ws.size());
-    for (size_t k = 0; k < ws.size(); k++) { timing[k] = ws[k]->log.timing; ws[k]->log.timing = false; }
-    const long long before = launches();
-    TOMO_CUDA(cudaStreamBeginCapture(W0().main, cudaStreamCaptureModeThreadLocal));
-    int rc = fork();
+    const bool timing = W.log.timing;
+    long long before = 0;
+    for (long long c : W.log.launches) before += c;
+    W.log.timing = false;
+    TOMO_CUDA(cudaStreamBeginCapture(W.main, cudaStreamCaptureModeThreadLocal));
+    int rc = 0;
     for (int m : order)
-      if (rc == 0) rc = meshes[m]->sweep_device();
-    if (rc == 0) rc = join();
+      if ((rc = meshes[m]->sweep_device()) != 0) break;
     cudaGraph_t g = nullptr;
-    const cudaError_t e = cudaStreamEndCapture(W0().main, &g);
-    for (size_t k = 0; k < ws.size(); k++) ws[k]->log.timing = timing[k] != 0;
-    graph_kernels = launches() - before;
+    const cudaError_t e = cudaStreamEndCapture(W.main, &g);
+    W.log.timing = timing;
+    long long after = 0;
+    for (long long c : W.log.launches) after += c;
+    graph_kernels = after - before;
     if (rc) { if (g) cudaGraphDestroy(g); return rc; }
     if (e != cudaSuccess) return set_error(TOMO_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
     graph = g;
@@ -2115,33 +2052,26 @@ struct MultiEngine {
       rc = capture();
       graph_ptrs = buffer_addresses();
     }
-    if (rc == 0 && cudaEventRecord(a, W0().main) != cudaSuccess) rc = set_error(TOMO_ERR_CUDA, "event record");
+    if (rc == 0 && cudaEventRecord(a, W.main) != cudaSuccess) rc = set_error(TOMO_ERR_CUDA, "event record");
     if (rc == 0) {
       if (use_graph) {
-        const cudaError_t e = cudaGraphLaunch(exec, W0().main);
+        const cudaError_t e = cudaGraphLaunch(exec, W.main);
         if (e != cudaSuccess) rc = set_error(TOMO_ERR_CUDA, std::string("cudaGraphLaunch: ") + cudaGetErrorString(e));
       } else {
-        rc = fork();
         for (int m : order)
-          if (rc == 0) rc = meshes[m]->sweep_device();
-        if (rc == 0) rc = join();
+          if ((rc = meshes[m]->sweep_device()) != 0) break;
       }
     }
-    // the sweep alone (graph) ends at g; every workspace's stream waits for
-    // it, the re-runs of flagged orientations follow per mesh on its
-    // workspace's stream, and b marks every mesh resolved
+    // the sweep alone (graph) ends at g; the re-runs of flagged orientations
+    // follow per mesh on the same stream, and b marks every mesh resolved
     cudaEvent_t g = nullptr;
-    if (rc == 0 && (cudaEventCreate(&g) != cudaSuccess || cudaEventRecord(g, W0().main) != cudaSuccess))
+    if (rc == 0 && (cudaEventCreate(&g) != cudaSuccess || cudaEventRecord(g, W.main) != cudaSuccess))
       rc = set_error(TOMO_ERR_CUDA, "event record");
-    for (size_t k = 1; k < ws.size() && rc == 0; k++)
-      if (cudaStreamWaitEvent(ws[k]->main, g, 0) != cudaSuccess) rc = set_error(TOMO_ERR_CUDA, "stream wait");
     for (auto* e : meshes)
       if (rc == 0) rc = e->resolve();
-    for (size_t k = 1; k < ws.size() && rc == 0; k++)
-      if (cudaStreamSynchronize(ws[k]->main) != cudaSuccess) rc = set_error(TOMO_ERR_CUDA, "stream sync");
     float ms = 0.f, gms = 0.f;
     if (rc == 0) {
-      if (cudaEventRecord(b, W0().main) != cudaSuccess || cudaEventSynchronize(b) != cudaSuccess ||
+      if (cudaEventRecord(b, W.main) != cudaSuccess || cudaEventSynchronize(b) != cudaSuccess ||
           cudaEventElapsedTime(&ms, a, b) != cudaSuccess || cudaEventElapsedTime(&gms, a, g) != cudaSuccess)
         rc = set_error(TOMO_ERR_CUDA, "batch timing");
     }
