@@ -352,34 +352,6 @@ __device__ __forceinline__ BinRange unpack_range(unsigned v)
   return r;
 }
 
-// Adds `n` to counter[s] for every strip s of `r` with one shared atomic per
-// distinct strip range in the warp: the triangles of a warp are consecutive
-// and mostly fall in the same strip, so per-lane atomics on the same counter
-// would serialise.  Returns, per strip of the lane's range, nothing; the
-// lane's rank among the warp's lanes with the same range is `rank` and the
-// leader's pre-add values are broadcast in base[0..2] (ranges span at most
-// three strips here; wider ones fall back to per-lane atomics, flagged by
-// the return value false).
-__device__ __forceinline__ bool warp_range_add(int* counter, const BinRange& r, int& rank, int base[3])
-{
-  const int lane = threadIdx.x & 31;
-  const unsigned key = (r.s1 >= r.s0 && r.s1 - r.s0 < 3) ? ((unsigned)r.s0 | ((unsigned)(r.s1 - r.s0) << 16)) : 0xFFFFFFFFu;
-  const unsigned peers = __match_any_sync(0xFFFFFFFFu, key);
-  const int leader = __ffs(peers) - 1;
-  rank = __popc(peers & ((1u << lane) - 1u));
-  int b0 = 0, b1 = 0, b2 = 0;
-  if (key != 0xFFFFFFFFu && lane == leader) {
-    const int m = __popc(peers);
-    b0 = atomicAdd(&counter[r.s0], m);
-    if (r.s1 > r.s0) b1 = atomicAdd(&counter[r.s0 + 1], m);
-    if (r.s1 > r.s0 + 1) b2 = atomicAdd(&counter[r.s0 + 2], m);
-  }
-  base[0] = __shfl_sync(0xFFFFFFFFu, b0, leader);
-  base[1] = __shfl_sync(0xFFFFFFFFu, b1, leader);
-  base[2] = __shfl_sync(0xFFFFFFFFu, b2, leader);
-  return key != 0xFFFFFFFFu || r.s1 < r.s0;
-}
-
 __global__ void __launch_bounds__(256) k_bin_count(EngineParams p)
 {
   extern __shared__ int sh_cnt[];
@@ -397,9 +369,7 @@ __global__ void __launch_bounds__(256) k_bin_count(EngineParams p)
       r = bin_range(p, o, t, sh, &sflag, nullptr);
       p.trange[(size_t)o * p.nT + t] = pack_range(r);
     }
-    int rank, base[3];
-    if (!warp_range_add(sh_cnt, r, rank, base))
-      for (int s = r.s0; s <= r.s1; s++) atomicAdd(&sh_cnt[s], 1);
+    for (int s = r.s0; s <= r.s1; s++) atomicAdd(&sh_cnt[s], 1);
   }
   __syncthreads();
   for (int s = threadIdx.x; s < p.S; s += blockDim.x)
@@ -455,9 +425,7 @@ __global__ void __launch_bounds__(256) k_bin_fill(EngineParams p)
     const int t = tb + threadIdx.x;
     BinRange r; r.s0 = 0; r.s1 = -1; r.code = 0;
     if (t < p.nT) r = unpack_range(tr[t]);
-    int rank, base[3];
-    if (!warp_range_add(lc, r, rank, base))
-      for (int s = r.s0; s <= r.s1; s++) atomicAdd(&lc[s], 1);
+    for (int s = r.s0; s <= r.s1; s++) atomicAdd(&lc[s], 1);
   }
   __syncthreads();
   for (int s = threadIdx.x; s < p.S; s += blockDim.x) {
@@ -471,10 +439,8 @@ __global__ void __launch_bounds__(256) k_bin_fill(EngineParams p)
     const int t = tb + threadIdx.x;
     BinRange r; r.s0 = 0; r.s1 = -1; r.code = 0;
     if (t < p.nT) r = unpack_range(tr[t]);
-    int rank, wb[3];
-    const bool grouped = warp_range_add(lc, r, rank, wb);
     for (int s = r.s0; s <= r.s1; s++) {
-      const int pos = off[s] + base[s] + (grouped ? wb[s - r.s0] + rank : atomicAdd(&lc[s], 1));
+      const int pos = off[s] + base[s] + atomicAdd(&lc[s], 1);
       if (pos < p.bin_cap) bins[pos] = t | ((r.code == 2) ? (int)0x80000000 : 0);
     }
   }
@@ -1010,13 +976,7 @@ __device__ __forceinline__ void exact_item(const EngineParams& p, const StripSme
   const float w = __fdiv_rn(wn, r.b.denom);
   const float u = __double2float_rn(__dsub_rn(__dsub_rn(1.0, (double)v), (double)w));
   if (!((u >= -0.001f) && (v >= -0.001f) && (v <= vmax) && (__fadd_rn(u, v) <= vmax))) return;
-  {
-    // mark the triangle as hit: one shared atomic per distinct word among the
-    // warp's hitting lanes (they mostly share a few triangles)
-    const unsigned peers = __match_any_sync(__activemask(), ti >> 5);
-    const unsigned bits = __reduce_or_sync(peers, 1u << (ti & 31));
-    if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicOr(&sm.thit[ti >> 5], bits);
-  }
+  atomicOr(&sm.thit[ti >> 5], 1u << (ti & 31));
   const float fx = bary3(r.ax, r.bx, r.cx, u, v, w);
   const float fy = bary3(r.ay, r.by, r.cy, u, v, w);
   const float fz = bary3(r.az, r.bz, r.cz, u, v, w);
