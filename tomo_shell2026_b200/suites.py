@@ -116,7 +116,7 @@ def coarse_interpolation(vss: np.ndarray, n_yaw: int, n_pitch: int, stride: int)
 
 
 def surrogate_suite(n_meshes: int = 100, seed0: int = 1000, stride: int = 10, cell: int = 5, top_k: int = 64,
-                    steps: int = 200, ratio_target: float = 0.2, margin: float = 1.0, holdout: float = 0.0,
+                    steps: int = 300, ratio_target: float = 0.2, margin: float = 1.0, holdout: float = 0.0,
                     lr: float = 3e-3, max_eval: int = -1, log_scale: float = 0.3, ablation: bool = True) -> dict:
     """The learned-proposal search against the exhaustive sweep on the same
     meshes, and (``ablation``) the same search without the network -- blocks

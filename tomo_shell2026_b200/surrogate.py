@@ -87,7 +87,7 @@ class SearchResult:
 
 
 def search(mesh, ypr, n_yaw: int, n_pitch: int, opts, stride: int = 10, cell: int = 5, top_k: int = 64,
-           steps: int = 200, lr: float = 3e-3, seed: int = 0, max_eval: int = -1, gate: float = 0.5,
+           steps: int = 300, lr: float = 3e-3, seed: int = 0, max_eval: int = -1, gate: float = 0.5,
            margin: float = 1.0, holdout: float = 0.0, log_scale: float = 0.3,
            proposal: str = "network") -> SearchResult:
     """Learned-proposal search over ypr = grid [n_pitch][n_yaw] (yaw fastest):
