@@ -207,7 +207,8 @@ __device__ __forceinline__ T warp_sum(T v)
   return v;
 }
 
-// Block-wide exclusive scan of one int per thread (blockDim.x == 256).
+// Block-wide exclusive scan of one int per thread (blockDim.x == 256).  Two
+// consecutive calls must be separated by a __syncthreads().
 __device__ __forceinline__ int block_excl_scan(int v, int* warp_tot, int& total)
 {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -229,7 +230,8 @@ __device__ __forceinline__ int block_excl_scan(int v, int* warp_tot, int& total)
   __syncthreads();
   const int before = (wid > 0) ? warp_tot[wid - 1] : 0;
   total = warp_tot[nw - 1];
-  __syncthreads();
+  // no barrier here: every caller reaches another __syncthreads() before
+  // the next call writes warp_tot again
   return before + x - v;
 }
 
@@ -471,7 +473,7 @@ struct StripSmem {
   float4* q0; float4* q1; float4* q2;   // [kChunk] margined vertices, vertex-normal z
   int4* tm;            // [kChunk] t, x0, y0, ylen
   int* pref;           // [kChunk + 4]
-  unsigned* thit;      // [kChunk / 32] triangles with an accepted pixel
+  unsigned* thit;      // [2][kChunk / 32] triangles with an accepted pixel, by chunk parity
   uint8_t* tkind;      // [kChunk] bit 0: fallback only; bit 1: box inside one strip
   float* fbz;          // [kChunk] z of each staged triangle's centroid fallback pixel
   unsigned* wq;        // [warps][kWalkQueue] pixels past the pre-reject, per warp
@@ -485,7 +487,7 @@ struct StripSmem {
 
 __host__ __device__ inline size_t strip_chunk_bytes()
 {
-  return 3 * sizeof(float4) * kChunk + sizeof(int4) * kChunk + sizeof(int) * (kChunk + 4) + sizeof(unsigned) * (kChunk / 32) +
+  return 3 * sizeof(float4) * kChunk + sizeof(int4) * kChunk + sizeof(int) * (kChunk + 4) + 2 * sizeof(unsigned) * (kChunk / 32) +
          sizeof(float) * kChunk + sizeof(unsigned) * kWalkQueue * (kChunk / 32) + kChunk;
 }
 
@@ -1026,7 +1028,8 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 1) k_strip(EngineParams p
   sm.q2 = (float4*)q; q += sizeof(float4) * kChunk;
   sm.tm = (int4*)q; q += sizeof(int4) * kChunk;
   sm.pref = (int*)q; q += sizeof(int) * (kChunk + 4);
-  sm.thit = (unsigned*)q; q += sizeof(unsigned) * (kChunk / 32);
+  unsigned* const thit_base = (unsigned*)q; q += 2 * sizeof(unsigned) * (kChunk / 32);
+  sm.thit = thit_base;
   sm.fbz = (float*)q; q += sizeof(float) * kChunk;
   sm.wq = (unsigned*)q; q += sizeof(unsigned) * kWalkQueue * (kChunk / 32);
   sm.tkind = (uint8_t*)q; q += kChunk;
@@ -1056,15 +1059,42 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 1) k_strip(EngineParams p
   const float half = p.half, vmax = p.vmax;
 
   // ---- phase A: rasterize the strip's triangles into shared memory
-  for (int cb = 0; cb < nlist; cb += kChunk) {
+  // The centroid fallback of a chunk's triangles runs at the start of the
+  // next chunk (before the same thread stages the next triangle into the
+  // same slot), so it needs no barrier of its own; the hit marks alternate
+  // between two buffers so that the next chunk can clear its own meanwhile.
+  int prev_n = 0;                                  // triangles of the chunk whose fallback is pending
+  int fb_xy = 0;                                   // its centroid slot (priority and safe strips)
+  auto fallback = [&](int n_prev, const unsigned* hit) {
+    const int i = threadIdx.x;
+    if (i >= n_prev) return;
+    const int kind = sm.tkind[i];
+    const bool fb = (kind & 1) || ((kind & 2) && ((hit[i >> 5] >> (i & 31)) & 1u) == 0u);
+    if (!fb) return;
+    const float n0 = sm.q0[i].w;
+    const int tx = sm.tm[i].x;
+    const unsigned t = MODE == 0 ? 0u : (unsigned)tx;   // the priority is only read by priority strips
+    const int xy = MODE == 0 ? tx : fb_xy;
+    const int sx = (int)(short)(xy & 0xFFFF), sy = xy >> 16;
+    const float fb_z = sm.fbz[i];
+    emit<MODE>(p, sm, &nent, &sflag, xs0, xs1, sx, sy, to_i16(fb_z), to_i16(__fmul_rn(n0, 1000.0f)), t, 0u);
+    if (p.twin) {
+      const float fz2 = __fadd_rn(fb_z, (n0 >= 0.0f) ? -p.shell_off : p.shell_off);
+      emit<MODE>(p, sm, &nent, &sflag, xs0, xs1, sx, sy, to_i16(fz2), to_i16(__fmul_rn(-n0, 1000.0f)), t, 1u);
+    }
+  };
+  int chunk_no = 0;
+  for (int cb = 0; cb < nlist; cb += kChunk, chunk_no++) {
     const int i = threadIdx.x;
     const int nchunk = min(kChunk, nlist - cb);
+    if (prev_n) fallback(prev_n, thit_base + ((chunk_no + 1) & 1) * (kChunk / 32));
+    sm.thit = thit_base + (chunk_no & 1) * (kChunk / 32);
     int npix = 0;
     // centroid fallback pixel of this thread's triangle (STomoSh_INT3.cpp:1190-1206), from the
     // translated unmargined vertices while they are in registers; used after the walk if the
     // triangle had no accepted pixel: slot x, y packed as two int16 (normal strips keep them in
     // the staged triangle record, whose triangle index only priority strips read), and z (fbz)
-    int fb_xy = 0;
+    fb_xy = 0;
     if (i < nchunk) {
       const int entry = list[cb + i];
       const int t = entry & 0x7FFFFFFF;
@@ -1109,6 +1139,8 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 1) k_strip(EngineParams p
     // warp runs the exact barycentric test and the pixel's emission on one
     // of them -- so the divisions, the double-precision u and the append run
     // on full warps instead of on the few lanes whose item passed.
+    // the next chunk's bin entries head for L2 while this chunk is walked
+    if (cb + kChunk + i < nlist) asm volatile("prefetch.global.L2 [%0];" ::"l"(list + cb + kChunk + i));
     const int per = (total + blockDim.x - 1) / blockDim.x;   // CTA-uniform trip count
     const int j0 = min(i * per, total), j1 = min(j0 + per, total);
     const int lane = i & 31;
@@ -1187,26 +1219,10 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 1) k_strip(EngineParams p
     __syncwarp();
     if (lane < qn) exact_item<MODE>(p, sm, &nent, &sflag, xs0, xs1, xlo, wq[lane], half, vmax);
     __syncthreads();
-    // centroid fallback of triangles without any accepted pixel
-    if (i < nchunk) {
-      const int kind = sm.tkind[i];
-      const bool fb = (kind & 1) || ((kind & 2) && ((sm.thit[i >> 5] >> (i & 31)) & 1u) == 0u);
-      if (fb) {
-        const float n0 = sm.q0[i].w;
-        const int tx = sm.tm[i].x;
-        const unsigned t = MODE == 0 ? 0u : (unsigned)tx;   // the priority is only read by priority strips
-        const int xy = MODE == 0 ? tx : fb_xy;
-        const int sx = (int)(short)(xy & 0xFFFF), sy = xy >> 16;
-        const float fb_z = sm.fbz[i];
-        emit<MODE>(p, sm, &nent, &sflag, xs0, xs1, sx, sy, to_i16(fb_z), to_i16(__fmul_rn(n0, 1000.0f)), t, 0u);
-        if (p.twin) {
-          const float fz2 = __fadd_rn(fb_z, (n0 >= 0.0f) ? -p.shell_off : p.shell_off);
-          emit<MODE>(p, sm, &nent, &sflag, xs0, xs1, sx, sy, to_i16(fz2), to_i16(__fmul_rn(-n0, 1000.0f)), t, 1u);
-        }
-      }
-    }
-    __syncthreads();
+    prev_n = nchunk;
   }
+  if (prev_n) fallback(prev_n, thit_base + ((chunk_no + 1) & 1) * (kChunk / 32));
+  __syncthreads();
 
   // ---- occupied slots in slot order (bitmap from the list heads -> list)
   const int wl = (HGs + 31) >> 5;
