@@ -155,10 +155,14 @@ __device__ __forceinline__ float centroid(float a, float b, float c)
   return __fadd_rn(__fmul_rn(__fadd_rn(__fadd_rn(a, b), c), 0.333333f), 0.001f);
 }
 
-// Whether any pixel centre of the box passes the barycentric test.  Pixels
-// whose sign-adjusted numerators lie outside the acceptance box by twice the
-// 0.001 margin are rejected before the divisions (the same pre-reject as the
-// strip walk; every such pixel fails the exact test too).  The pixel nearest
+// Whether any pixel centre of the box passes the barycentric test.  Per
+// pixel the sign-adjusted numerators of v and w (the exact test's own float
+// values) decide most cases without a division: outside the acceptance
+// region by twice the 0.001 margin (v or w out of range, or v + w past 1)
+// the pixel fails the exact test too; with v, w >= 0 and v + w below
+// 1 - 1e-6 it passes (then v, w >= 0 and v + w < 1 after the divisions, so
+// u >= 0 and u + v <= 1 + 2^-23, inside every bound of the test).  Only
+// pixels in the thin band between run the exact test.  The pixel nearest
 // the centroid is tried first: for all but the smallest triangles it is
 // inside, and the box scan is skipped.
 __device__ bool any_hit(const EngineParams& p, const TriGeo& g, const Bary& b)
@@ -167,29 +171,37 @@ __device__ bool any_hit(const EngineParams& p, const TriGeo& g, const Bary& b)
   const float ad = b.denom >= 0.0f ? b.denom : -b.denom;
   const bool dpos = b.denom > 0.0f;
   const float rlo = __fmul_rn(-0.002f, ad), rvhi = __fmul_rn(1.002f, ad), rwhi = __fmul_rn(1.004f, ad);
+  const float ruhi = __fmul_rn(1.003f, ad), rin = __fmul_rn(0.999999f, ad);
+  // 0: rejected, 1: accepted, 2: needs the exact test
+  auto classify = [&](float px, float py) {
+    const float e2x = __fsub_rn(px, g.ax), e2y = __fsub_rn(py, g.ay);
+    const float d20 = dot2(e2x, e2y, b.e0x, b.e0y);
+    const float d21 = dot2(e2x, e2y, b.e1x, b.e1y);
+    const float vn = __fsub_rn(__fmul_rn(b.d11, d20), __fmul_rn(b.d01, d21));
+    const float wn = __fsub_rn(__fmul_rn(b.d00, d21), __fmul_rn(b.d01, d20));
+    const float vs = dpos ? vn : -vn, ws = dpos ? wn : -wn;
+    const float sum = __fadd_rn(vs, ws);
+    if (vs < rlo || vs > rvhi || ws < rlo || ws > rwhi || sum > ruhi) return 0;
+    if (vs >= 0.0f && ws >= 0.0f && sum <= rin) return 1;
+    return 2;
+  };
+  auto hit = [&](int x, int y) {
+    const float px = pix_center(x, p.half), py = pix_center(y, p.half);
+    const int c = classify(px, py);
+    if (c != 2) return c == 1;
+    float u, v, w;
+    return bary_test(g.ax, g.ay, b, px, py, p.vmax, u, v, w);
+  };
   {
     // a guess only (any pixel of the box would do), so its rounding does not matter
     const float mx = (g.ax + g.bx + g.cx) * (1.0f / 3.0f), my = (g.ay + g.by + g.cy) * (1.0f / 3.0f);
     const int x = min(max(__float2int_rd(mx - p.half), g.x0), g.x1);
     const int y = min(max(__float2int_rd(my - p.half), g.y0), g.y1);
-    float u, v, w;
-    if (bary_test(g.ax, g.ay, b, pix_center(x, p.half), pix_center(y, p.half), p.vmax, u, v, w)) return true;
+    if (hit(x, y)) return true;
   }
-  for (int x = g.x0; x <= g.x1; x++) {
-    const float px = pix_center(x, p.half);
-    const float e2x = __fsub_rn(px, g.ax);
-    for (int y = g.y0; y <= g.y1; y++) {
-      const float e2y = __fsub_rn(pix_center(y, p.half), g.ay);
-      const float d20 = dot2(e2x, e2y, b.e0x, b.e0y);
-      const float d21 = dot2(e2x, e2y, b.e1x, b.e1y);
-      const float vn = __fsub_rn(__fmul_rn(b.d11, d20), __fmul_rn(b.d01, d21));
-      const float wn = __fsub_rn(__fmul_rn(b.d00, d21), __fmul_rn(b.d01, d20));
-      const float vs = dpos ? vn : -vn, ws = dpos ? wn : -wn;
-      if (vs < rlo || vs > rvhi || ws < rlo || ws > rwhi) continue;
-      float u, v, w;
-      if (bary_test(g.ax, g.ay, b, px, pix_center(y, p.half), p.vmax, u, v, w)) return true;
-    }
-  }
+  for (int x = g.x0; x <= g.x1; x++)
+    for (int y = g.y0; y <= g.y1; y++)
+      if (hit(x, y)) return true;
   return false;
 }
 
