@@ -155,28 +155,25 @@ __device__ __forceinline__ float centroid(float a, float b, float c)
   return __fadd_rn(__fmul_rn(__fadd_rn(__fadd_rn(a, b), c), 0.333333f), 0.001f);
 }
 
-// Whether a pixel centre passes the barycentric test, from the exact test's
-// own float numerators of v and w where they decide it without a division:
-// outside the acceptance region by twice the 0.001 margin (v or w out of
-// range, or v + w past 1) the pixel fails the exact test too; with v, w >= 0
-// and v + w below 1 - 1e-6 it passes (then v, w >= 0 and v + w < 1 after the
-// divisions, so u >= 0 and u + v <= 1 + 2^-23, inside every bound of the
-// test).  Only pixels in the thin band between run the exact test.
-struct HitTest {
-  const TriGeo& g;
-  const Bary& b;
-  float half, vmax, ad, rlo, rvhi, rwhi, ruhi, rin;
-  bool dpos;
-  __device__ HitTest(const TriGeo& g_, const Bary& b_, float half_, float vmax_) : g(g_), b(b_), half(half_), vmax(vmax_)
-  {
-    ad = b.denom >= 0.0f ? b.denom : -b.denom;
-    dpos = b.denom > 0.0f;
-    rlo = __fmul_rn(-0.002f, ad); rvhi = __fmul_rn(1.002f, ad); rwhi = __fmul_rn(1.004f, ad);
-    ruhi = __fmul_rn(1.003f, ad); rin = __fmul_rn(0.999999f, ad);
-  }
-  __device__ bool pixel(int x, int y) const
-  {
-    const float px = pix_center(x, half), py = pix_center(y, half);
+// Whether any pixel centre of the box passes the barycentric test.  Per
+// pixel the sign-adjusted numerators of v and w (the exact test's own float
+// values) decide most cases without a division: outside the acceptance
+// region by twice the 0.001 margin (v or w out of range, or v + w past 1)
+// the pixel fails the exact test too; with v, w >= 0 and v + w below
+// 1 - 1e-6 it passes (then v, w >= 0 and v + w < 1 after the divisions, so
+// u >= 0 and u + v <= 1 + 2^-23, inside every bound of the test).  Only
+// pixels in the thin band between run the exact test.  The pixel nearest
+// the centroid is tried first: for all but the smallest triangles it is
+// inside, and the box scan is skipped.
+__device__ bool any_hit(const EngineParams& p, const TriGeo& g, const Bary& b)
+{
+  if (!b.ok) return false;
+  const float ad = b.denom >= 0.0f ? b.denom : -b.denom;
+  const bool dpos = b.denom > 0.0f;
+  const float rlo = __fmul_rn(-0.002f, ad), rvhi = __fmul_rn(1.002f, ad), rwhi = __fmul_rn(1.004f, ad);
+  const float ruhi = __fmul_rn(1.003f, ad), rin = __fmul_rn(0.999999f, ad);
+  // 0: rejected, 1: accepted, 2: needs the exact test
+  auto classify = [&](float px, float py) {
     const float e2x = __fsub_rn(px, g.ax), e2y = __fsub_rn(py, g.ay);
     const float d20 = dot2(e2x, e2y, b.e0x, b.e0y);
     const float d21 = dot2(e2x, e2y, b.e1x, b.e1y);
@@ -184,32 +181,36 @@ struct HitTest {
     const float wn = __fsub_rn(__fmul_rn(b.d00, d21), __fmul_rn(b.d01, d20));
     const float vs = dpos ? vn : -vn, ws = dpos ? wn : -wn;
     const float sum = __fadd_rn(vs, ws);
-    if (vs < rlo || vs > rvhi || ws < rlo || ws > rwhi || sum > ruhi) return false;
-    if (vs >= 0.0f && ws >= 0.0f && sum <= rin) return true;
+    if (vs < rlo || vs > rvhi || ws < rlo || ws > rwhi || sum > ruhi) return 0;
+    if (vs >= 0.0f && ws >= 0.0f && sum <= rin) return 1;
+    return 2;
+  };
+  auto hit = [&](int x, int y) {
+    const float px = pix_center(x, p.half), py = pix_center(y, p.half);
+    const int c = classify(px, py);
+    if (c != 2) return c == 1;
     float u, v, w;
-    return bary_test(g.ax, g.ay, b, px, py, vmax, u, v, w);
-  }
-  // The pixel nearest the centroid: for all but the smallest triangles it is
-  // inside.  (A guess only -- any pixel of the box would do -- so its
-  // rounding does not matter.)
-  __device__ bool centroid_pixel() const
+    return bary_test(g.ax, g.ay, b, px, py, p.vmax, u, v, w);
+  };
   {
+    // a guess only (any pixel of the box would do), so its rounding does not matter
     const float mx = (g.ax + g.bx + g.cx) * (1.0f / 3.0f), my = (g.ay + g.by + g.cy) * (1.0f / 3.0f);
-    const int x = min(max(__float2int_rd(mx - half), g.x0), g.x1);
-    const int y = min(max(__float2int_rd(my - half), g.y0), g.y1);
-    return pixel(x, y);
+    const int x = min(max(__float2int_rd(mx - p.half), g.x0), g.x1);
+    const int y = min(max(__float2int_rd(my - p.half), g.y0), g.y1);
+    if (hit(x, y)) return true;
   }
-  // Any pixel of the box in columns [x0, x1] outside [skip0, skip1].
-  __device__ bool columns(int x0, int x1, int skip0, int skip1) const
-  {
-    for (int x = x0; x <= x1; x++) {
-      if (x >= skip0 && x <= skip1) continue;
-      for (int y = g.y0; y <= g.y1; y++)
-        if (pixel(x, y)) return true;
-    }
-    return false;
-  }
-};
+  for (int x = g.x0; x <= g.x1; x++)
+    for (int y = g.y0; y <= g.y1; y++)
+      if (hit(x, y)) return true;
+  return false;
+}
+
+// Slot x of the centroid fallback pixel.
+__device__ __forceinline__ int centroid_slot_x(const float4* raw, const Shift& sh)
+{
+  const float ux = centroid(__fsub_rn(raw[0].x, sh.dx), __fsub_rn(raw[1].x, sh.dx), __fsub_rn(raw[2].x, sh.dx));
+  return __float2int_rz(ux);
+}
 
 template <typename T>
 __device__ __forceinline__ T warp_sum(T v)
@@ -303,18 +304,16 @@ __global__ void __launch_bounds__(256) k_rotate(EngineParams p)
 
 // ---------------------------------------------------------------- K2 binning
 // Strip range of one triangle.  Normal mode: the strips its pixel box
-// covers.  A triangle spanning several strips needs its centroid fallback
-// (triVoxel's, STomoSh_INT3.cpp:1190-1206) only if no pixel of its whole
-// box is a hit; when the pixel nearest its centroid is a hit that is settled
-// here (code 1), otherwise it is left to the strip of its centroid pixel,
-// which scans the box's other columns if its own had no hit (code 3,
-// "undecided", carried in the bin entry's sign bit).  Safe mode: the box
-// widened by e columns on both sides, since in safe mode a strip evaluates
-// every pixel of every triangle whose hits could reach it.
+// covers; a triangle spanning several strips whose box holds no accepted
+// pixel centre goes only to the strip of its centroid pixel, flagged as
+// "fallback only" (code 2).  Safe mode: the box widened by e columns on both
+// sides, since in safe mode a strip evaluates every pixel of every triangle
+// whose hits could reach it.
 
 struct BinRange { int s0, s1, code; };
 
-__device__ __forceinline__ BinRange bin_range(const EngineParams& p, int o, int t, const Shift& sh, int* flag)
+__device__ __forceinline__ BinRange bin_range(const EngineParams& p, int o, int t, const Shift& sh, int* flag,
+                                              const uint8_t* known_code)
 {
   TriGeo g;
   float4 raw[3];
@@ -327,9 +326,19 @@ __device__ __forceinline__ BinRange bin_range(const EngineParams& p, int o, int 
     r.s0 = min(x0 / p.H, p.S - 1);
     r.s1 = min(max(x1, 0) / p.H, p.S - 1);
     if (r.s0 != r.s1) {
-      Bary b;
-      bary_setup(g, b);
-      r.code = (b.ok && HitTest(g, b, p.half, p.vmax).centroid_pixel()) ? 1 : 3;
+      int code;
+      if (known_code) code = *known_code;
+      else {
+        Bary b;
+        bary_setup(g, b);
+        code = any_hit(p, g, b) ? 1 : 2;
+      }
+      r.code = code;
+      if (code == 2) {
+        const int cxs = centroid_slot_x(raw, sh);
+        const int sc = min(max(cxs, 0), p.G - 1) / p.H;
+        r.s0 = r.s1 = min(sc, p.S - 1);
+      }
     }
   } else {
     const float xmin = fmin_ref(fmin_ref(g.ax, g.bx), g.cx);
@@ -371,7 +380,7 @@ __global__ void __launch_bounds__(256) k_bin_count(EngineParams p)
     const int t = tb + threadIdx.x;
     BinRange r; r.s0 = 0; r.s1 = -1; r.code = 0;
     if (t < p.nT) {
-      r = bin_range(p, o, t, sh, &sflag);
+      r = bin_range(p, o, t, sh, &sflag, nullptr);
       p.trange[(size_t)o * p.nT + t] = pack_range(r);
     }
     for (int s = r.s0; s <= r.s1; s++) atomicAdd(&sh_cnt[s], 1);
@@ -446,7 +455,7 @@ __global__ void __launch_bounds__(256) k_bin_fill(EngineParams p)
     if (t < p.nT) r = unpack_range(tr[t]);
     for (int s = r.s0; s <= r.s1; s++) {
       const int pos = off[s] + base[s] + atomicAdd(&lc[s], 1);
-      if (pos < p.bin_cap) bins[pos] = t | ((r.code == 3) ? (int)0x80000000 : 0);
+      if (pos < p.bin_cap) bins[pos] = t | ((r.code == 2) ? (int)0x80000000 : 0);
     }
   }
 }
@@ -477,7 +486,7 @@ struct StripSmem {
   int4* tm;            // [kChunk] t, x0, y0, ylen
   int* pref;           // [kChunk + 4]
   unsigned* thit;      // [2][kChunk / 32] triangles with an accepted pixel, by chunk parity
-  uint8_t* tkind;      // [kChunk] bit 0: spanning, hit undecided by binning; bit 1: box inside one strip
+  uint8_t* tkind;      // [kChunk] bit 0: fallback only; bit 1: box inside one strip
   float* fbz;          // [kChunk] z of each staged triangle's centroid fallback pixel
   unsigned* wq;        // [warps][kWalkQueue] pixels past the pre-reject, per warp
   short* olist;        // [H*G] occupied local slots in slot order (aliases the chunk area)
@@ -1072,25 +1081,13 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 1) k_strip(EngineParams p
     const int i = threadIdx.x;
     if (i >= n_prev) return;
     const int kind = sm.tkind[i];
-    if (!(kind & 3) || ((hit[i >> 5] >> (i & 31)) & 1u)) return;   // decided hit, or a hit in this strip
-    const int4 tm = sm.tm[i];
-    const unsigned t = MODE == 0 ? 0u : (unsigned)tm.x;   // the priority is only read by priority strips
-    const int xy = MODE == 0 ? tm.x : fb_xy;
-    const int sx = (int)(short)(xy & 0xFFFF), sy = xy >> 16;
-    if (!(kind & 2)) {
-      // spanning and undecided: only the strip of the centroid pixel decides,
-      // from the box's columns outside this strip
-      if (min(min(max(sx, 0), p.G - 1) / p.H, p.S - 1) != s) return;
-      const float4 a4 = sm.q0[i], b4 = sm.q1[i], c4 = sm.q2[i];
-      TriGeo g;
-      g.ax = a4.x; g.ay = a4.y; g.bx = b4.x; g.by = b4.y; g.cx = c4.x; g.cy = c4.y;
-      g.x0 = tm.y; g.y0 = tm.z; g.y1 = tm.z + tm.w - 1;
-      g.x1 = __float2int_rz(fmax_ref(fmax_ref(g.ax, g.bx), g.cx));
-      Bary b;
-      bary_setup(g, b);
-      if (b.ok && HitTest(g, b, half, vmax).columns(g.x0, g.x1, xs0, xs1 - 1)) return;
-    }
+    const bool fb = (kind & 1) || ((kind & 2) && ((hit[i >> 5] >> (i & 31)) & 1u) == 0u);
+    if (!fb) return;
     const float n0 = sm.q0[i].w;
+    const int tx = sm.tm[i].x;
+    const unsigned t = MODE == 0 ? 0u : (unsigned)tx;   // the priority is only read by priority strips
+    const int xy = MODE == 0 ? tx : fb_xy;
+    const int sx = (int)(short)(xy & 0xFFFF), sy = xy >> 16;
     const float fb_z = sm.fbz[i];
     emit<MODE>(p, sm, &nent, &sflag, xs0, xs1, sx, sy, to_i16(fb_z), to_i16(__fmul_rn(n0, 1000.0f)), t, 0u);
     if (p.twin) {
@@ -1113,7 +1110,7 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 1) k_strip(EngineParams p
     if (i < nchunk) {
       const int entry = list[cb + i];
       const int t = entry & 0x7FFFFFFF;
-      const int undecided = (entry < 0) ? 1 : 0;
+      const int fb_only = (entry < 0) ? 1 : 0;
       TriGeo g;
       float4 raw[3];
       load_tri(p, o, t, sh, g, raw);
@@ -1132,14 +1129,14 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 1) k_strip(EngineParams p
       if (MODE != 1) { xc0 = max(g.x0, xs0); xc1 = min(g.x1, xs1 - 1); }
       else { xc0 = g.x0; xc1 = g.x1; }
       const int ylen = g.y1 - g.y0 + 1;
-      if (b.ok && xc0 <= xc1 && ylen > 0) npix = (xc1 - xc0 + 1) * ylen;
-      // kind bit 0: spanning, hit undecided; bit 1: box inside one strip (local fallback decision)
+      if (!fb_only && b.ok && xc0 <= xc1 && ylen > 0) npix = (xc1 - xc0 + 1) * ylen;
+      // kind bit 0: fallback only; bit 1: box inside one strip (local fallback decision)
       const int single = (MODE == 1) || (min(max(g.x0, 0) / p.H, p.S - 1) == min(max(g.x1, 0) / p.H, p.S - 1));
       sm.q0[i] = make_float4(g.ax, g.ay, g.az, g.n0);
       sm.q1[i] = make_float4(g.bx, g.by, g.bz, g.n1);
       sm.q2[i] = make_float4(g.cx, g.cy, g.cz, g.n2);
       sm.tm[i] = make_int4(MODE == 0 ? fb_xy : t, g.x0, g.y0, ylen);
-      sm.tkind[i] = (uint8_t)(undecided | (single << 1));
+      sm.tkind[i] = (uint8_t)(fb_only | (single << 1));
     }
     if (i < kChunk / 32) sm.thit[i] = 0u;
     int total;
