@@ -324,6 +324,9 @@ struct Engine {
   DevBuf<long long> o_vo, o_vss, o_vtc, o_ent, o_col;
   DevBuf<float> o_vof, o_vssf, o_vtcf;
   DevBuf<int> o_nbed, o_flags;
+  // learned-proposal search: orientations, network features and
+  // predictions of the grid, kept between searches (they only grow)
+  DevBuf<float> srch_ypr, srch_x, srch_y;
   // subset fetch (see fetch_subset) and lazy rotations (see ensure_rot)
   DevBuf<int> sub_ids;
   DevBuf<long long> sub_stage;
@@ -364,6 +367,7 @@ struct Engine {
   {
     vpos.release(); vnrm.release(); tri.release(); rot.release(); ori.release();
     sub_ids.release(); sub_stage.release();
+    srch_ypr.release(); srch_x.release(); srch_y.release();
     o_vo.release(); o_vss.release(); o_vtc.release(); o_ent.release(); o_col.release();
     o_vof.release(); o_vssf.release(); o_vtcf.release(); o_nbed.release(); o_flags.release();
     if (owns_ws) W.release();
@@ -2427,7 +2431,10 @@ int tomoSurrogateSearch(const float* f32info, const int* i32info, const float* Y
       //    training and prediction); a seeded share of the coarse points is
       //    held out of training so the prediction error is also measured away
       //    from the refined cells; train on standardised exact Vss
-      DevBuf<float> dypr, dx, dy;
+      const auto t_feat = std::chrono::steady_clock::now();
+      DevBuf<float>& dypr = E.srch_ypr;
+      DevBuf<float>& dx = E.srch_x;
+      DevBuf<float>& dy = E.srch_y;
       TOMO_CUDA(dypr.reserve((size_t)n * 3));
       TOMO_CUDA(dx.reserve((size_t)n * kMlpIn));
       TOMO_CUDA(dy.reserve((size_t)n));
@@ -2436,6 +2443,7 @@ int tomoSurrogateSearch(const float* f32info, const int* i32info, const float* Y
       std::vector<float> F((size_t)n * kMlpIn);
       TOMO_CUDA(cudaMemcpyAsync(F.data(), dx.ptr, sizeof(float) * F.size(), cudaMemcpyDeviceToHost, E.main));
       TOMO_CUDA(cudaStreamSynchronize(E.main));
+      t_pred += seconds_since(t_feat);
       std::vector<int> train;
       {
         unsigned h = 2166136261u ^ (unsigned)seed;
@@ -2488,9 +2496,6 @@ int tomoSurrogateSearch(const float* f32info, const int* i32info, const float* Y
         }
         t_pred += seconds_since(t0);
       }
-      dypr.release();
-      dx.release();
-      dy.release();
     }
     // 4. cells by smallest prediction; refine the top_k
     std::vector<float> cmin(ncell, INFINITY);
