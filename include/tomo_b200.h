@@ -95,6 +95,8 @@ void tomoVolToMass(const float* f32info, const int* i32info, float* vm22);
 #define TOMO_OPT_PROPOSAL 7     /* tomoSurrogateSearch proposals: 0 = the trained network (default), 1 = bilinear
                                    interpolation of the exact coarse values (the search without the network),
                                    2 = the mean of the two */
+#define TOMO_OPT_FOLD_LIMIT 8   /* largest |column value| a packed 16-bit fold record holds (1..32767, default 32767);
+                                   larger values go through the batch's escape table.  Lower only to test that table */
 int tomoSetOption(int key, int value);
 
 /* out[0..8] = grid edge, strip height, strips, entry capacity, orientations re-run

@@ -166,6 +166,37 @@ def test_large_grid_solid(oracle):
     _compare(res, oracle.sweep(m, ypr, opts, grid=st["grid"]), "82k")
 
 
+@pytest.mark.parametrize("explicit_ss", [True, False])
+def test_fold_escape_table(oracle, explicit_ss):
+    """Fold records hold a column's (vo, vss, tc) as 16-bit values; a column
+    whose values do not fit goes through the batch's escape table.  Lowering
+    the record range so that a few hundred columns of one orientation escape
+    must leave every output bit unchanged (the 82k solid's Vo passes 2^24, so
+    its float fold is replayed column by column and reads those escapes); a
+    range of 1 overflows the table and must be an error, not a wrong sum."""
+    m = meshgen.solid_82k(0)
+    ypr = meshgen.ypr_grid(np.array([30.0]), np.array([40.0]))
+    opts = PrintOptions(explicit_ss=explicit_ss)
+    sess = native.Session(m, ypr, opts)
+    G = sess.grid()
+    cols = sess.columns(0)["cols"]
+    mag = np.sort(np.abs(cols[cols[:, 0] > 0, 2:5]).max(axis=1))[::-1]
+    lim = int(mag[600])
+    assert 1 <= lim < int(mag[0]) and np.count_nonzero(mag > lim) <= 600
+    want = oracle.sweep(m, ypr, opts, grid=G)
+    assert int(want["Vo64"][0]) > (1 << 24)
+    try:
+        native.set_option(native.TOMO_OPT_FOLD_LIMIT, lim)
+        res = native.sweep(m, ypr, opts)
+        _compare(res, want, f"limit {lim}")
+        native.set_option(native.TOMO_OPT_FOLD_LIMIT, 1)
+        with pytest.raises(native.TomoError, match="escape table"):
+            native.sweep(m, ypr, opts)
+    finally:
+        native.set_option(native.TOMO_OPT_FOLD_LIMIT, 32767)
+    _compare(native.sweep(m, ypr, opts), want, "default range")
+
+
 def test_bad_index_is_an_error():
     m = meshgen.small_solid(0)
     bad = meshgen.MeshArrays(m.vertices, m.faces.copy(), m.vertex_normals, m.face_normals, m.area)

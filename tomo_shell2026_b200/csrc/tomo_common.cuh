@@ -25,6 +25,15 @@ enum : int {
 
 enum : int { kBedNone = 0, kBedBrim = 1, kBedRaft = 2, kBedSkirt = 3 };
 
+// Fold records hold a column's (vo, vss) as two int16 and tc as one.  A
+// column whose values leave [-32767, 32767] (or the narrower range a test
+// asks for) writes the record kFoldEscaped
+// (both halves -32768, which no packed pair produces) and appends its exact
+// values, keyed by (orientation, record index), to the batch's escape table.
+struct FoldEscape { int o, pos, vo, vss, tc, pad0, pad1, pad2; };
+constexpr unsigned kFoldEscaped = 0x80008000u;
+constexpr int kFoldEscapes = 1024;
+
 // Per-orientation status bits.  The first three ask for the exact
 // safe-mode re-run of that orientation; the rest are hard errors.
 enum : int {
@@ -34,6 +43,7 @@ enum : int {
   kFlagGrid = 8,       // a slot index fell outside the grid (grid too small)
   kFlagSafeOverflow = 16,
   kFlagCap = 32,       // a column exceeded the 63-pixel cap: needs first-come priorities
+  kFlagFoldRange = 64, // column values past 16 bits overflowed the batch's escape table
 };
 // Results of an orientation flagged with any of these are not written.
 constexpr int kFlagRedo = kFlagStray | kFlagOverflow | kFlagBinCap | kFlagCap;
@@ -102,8 +112,11 @@ struct EngineParams {
   int* bbox;            // [Bo][4] min x, min y, max x, max y of occupied slots
   uint8_t* bedf;        // [Bo][G*G]
   int* foldcnt;         // [Bo][S]
-  int2* foldv;          // [Bo][G*G] (vo, vss) of each occupied column, in slot order per strip
-  int* foldtc;          // [Bo][G*G] tc of each occupied column (implicit support only, else null)
+  unsigned* foldp;      // [Bo][G*G] (vo, vss) of each occupied column as two int16, in slot order per strip
+  short* foldtc;        // [Bo][G*G] tc of each occupied column (implicit support only, else null)
+  FoldEscape* foldx;    // [kFoldEscapes] columns whose values do not fit 16 bits (record kFoldEscaped)
+  int* foldxn;          // entries appended to foldx in this batch
+  int fold_lim;         // largest |value| a packed record holds (32767; lower only to test the escape table)
   int* foldmeta;        // [Bo][S][8] per strip: sum vo, vss, tc, |vss|, |tc|
 
   // per-orientation outputs (indexed by orientation id)

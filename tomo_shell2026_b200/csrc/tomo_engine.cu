@@ -199,8 +199,10 @@ struct BatchSet {   // per-batch buffers read by the fold, double-buffered
   DevBuf<long long> acc;
   DevBuf<int> flags;
   DevBuf<int> foldcnt;
-  DevBuf<int2> foldv;
-  DevBuf<int> foldtc;
+  DevBuf<unsigned> foldp;
+  DevBuf<short> foldtc;
+  DevBuf<FoldEscape> foldx;
+  DevBuf<int> foldxn;
   DevBuf<int> foldmeta;
   cudaEvent_t folded = nullptr;
 };
@@ -261,7 +263,7 @@ struct Workspace {
   void release()
   {
     for (auto& q : prep) q.release();
-    for (auto& s : set) { s.acc.release(); s.flags.release(); s.foldcnt.release(); s.foldv.release(); s.foldtc.release(); s.foldmeta.release(); }
+    for (auto& s : set) { s.acc.release(); s.flags.release(); s.foldcnt.release(); s.foldp.release(); s.foldtc.release(); s.foldx.release(); s.foldxn.release(); s.foldmeta.release(); }
     dump_cols.release(); dump_keys.release(); dump_types.release();
     dump_off.release(); dump_tot.release(); dump_ccols.release(); dump_ckeys.release(); dump_ctypes.release();
     log.destroy();
@@ -344,6 +346,7 @@ struct Engine {
   int normal_smem = 0;    // shared-memory budget of a normal strip CTA (0 = four CTAs per SM)
   int export_pixels = 1;  // rebuild the best orientation's pixels and vm_info (TomoSh_CUDA tail)
   int adaptive = 1;       // raise the entry budget after overflowing early batches (full sweeps)
+  int fold_lim = 32767;   // largest |column value| of a packed fold record (TOMO_OPT_FOLD_LIMIT)
   int adapt_smem = 0, adapt_h = 0;   // configuration adapted to by an earlier sweep of this upload
   int adapt_cfg = 0;                  // 4 once a sweep of this upload switched to priority strips
   int start_cfg = 0;                  // 4: every sweep starts in priority strips (set by the batch autotuner)
@@ -530,6 +533,7 @@ struct Engine {
     p.out_vof = o_vof.ptr; p.out_vssf = o_vssf.ptr; p.out_vtcf = o_vtcf.ptr;
     p.out_nbed = o_nbed.ptr; p.out_flags = o_flags.ptr; p.out_entries = o_ent.ptr; p.out_columns = o_col.ptr;
     p.dump_slot = -1;
+    p.fold_lim = fold_lim;
     return p;
   }
 
@@ -551,8 +555,10 @@ struct Engine {
       TOMO_CUDA(s.acc.reserve((size_t)Bo * kAccLanes));
       TOMO_CUDA(s.flags.reserve((size_t)Bo));
       TOMO_CUDA(s.foldcnt.reserve((size_t)Bo * S));
-      TOMO_CUDA(s.foldv.reserve((size_t)Bo * GG));
+      TOMO_CUDA(s.foldp.reserve((size_t)Bo * GG));
       if (!P.explicit_ss) TOMO_CUDA(s.foldtc.reserve((size_t)Bo * GG));
+      TOMO_CUDA(s.foldx.reserve(kFoldEscapes));
+      TOMO_CUDA(s.foldxn.reserve(1));
       TOMO_CUDA(s.foldmeta.reserve((size_t)Bo * S * 8));
     }
     return 0;
@@ -577,8 +583,9 @@ struct Engine {
     p.bin_off = b.bin_off.ptr; p.bin_cur = b.bin_cur.ptr; p.bins = b.bins.ptr; p.bin_cap = bin_cap;
     p.bbox = b.bbox.ptr; p.bedf = b.bedf.ptr;
     p.acc = set[which].acc.ptr; p.flags = set[which].flags.ptr;
-    p.foldcnt = set[which].foldcnt.ptr; p.foldv = set[which].foldv.ptr; p.foldmeta = set[which].foldmeta.ptr;
+    p.foldcnt = set[which].foldcnt.ptr; p.foldp = set[which].foldp.ptr; p.foldmeta = set[which].foldmeta.ptr;
     p.foldtc = p.explicit_ss ? nullptr : set[which].foldtc.ptr;
+    p.foldx = set[which].foldx.ptr; p.foldxn = set[which].foldxn.ptr;
   }
 
   // All orientations in configuration 0, asynchronously on `main`.  With
@@ -898,6 +905,8 @@ struct Engine {
       if (flags[i] & kFlagSafeOverflow) return set_error(TOMO_ERR_CAPACITY, "column strip exceeds shared memory");
       if (flags[i] & kFlagGrid) return set_error(TOMO_ERR_CAPACITY, "slot index outside the grid");
       if (flags[i] & kFlagRedo) return set_error(TOMO_ERR_CAPACITY, "orientation unresolved after the re-runs");
+      if (flags[i] & kFlagFoldRange)
+        return set_error(TOMO_ERR_CAPACITY, "column values past 16 bits overflowed the fold escape table");
     }
     n_safe = n_redo[1] + n_redo[2] + n_redo[3] + n_redo[4];
     return 0;
@@ -1398,6 +1407,7 @@ int tomoSetOption(int key, int value)
     case TOMO_OPT_EXPORT: E.export_pixels = value ? 1 : 0; return 0;
     case TOMO_OPT_ADAPTIVE: E.adaptive = value ? 1 : 0; E.adapt_smem = E.adapt_h = E.adapt_cfg = 0; return 0;
     case TOMO_OPT_PROPOSAL: if (value < 0 || value > 2) return TOMO_ERR_ARG; g_proposal = value; return 0;
+    case TOMO_OPT_FOLD_LIMIT: if (value < 1 || value > 32767) return TOMO_ERR_ARG; E.fold_lim = value; return 0;
     default: return TOMO_ERR_ARG;
   }
 }
@@ -1595,7 +1605,8 @@ constexpr size_t static_bytes(size_t nV, size_t nT)
          static_round(16 * B * nV) + static_round(4 * 4 * B) + static_round(4 * B * nT) +
          static_round(4 * B * (S + 1)) + static_round(4 * B * S) + static_round(4 * B * (4 * nT + 4096)) +
          static_round(4 * 4 * B) + static_round(B * GG) + static_round(8 * B * kAccLanes) + static_round(4 * B) +
-         static_round(4 * B * S) + static_round(8 * B * GG) + static_round(4 * B * GG) + static_round(4 * B * S * 8) +
+         static_round(4 * B * S) + static_round(4 * B * GG) + static_round(2 * B * GG) + static_round(sizeof(FoldEscape) * kFoldEscapes) +
+         static_round(4) + static_round(4 * B * S * 8) +
          5 * static_round(8 * B) + 3 * static_round(4 * B) + 2 * static_round(4 * B);
 }
 static_assert(static_bytes(kStaticMaxVtx, kStaticMaxTri) <= kStaticArenaBytes,
@@ -1609,8 +1620,10 @@ struct StaticLayout {
   unsigned *minkey, *trange;
   uint8_t* bedf;
   long long *acc, *o_vo, *o_vss, *o_vtc, *o_ent, *o_col;
-  int2* foldv;
-  int* foldtc;
+  unsigned* foldp;
+  short* foldtc;
+  FoldEscape* foldx;
+  int* foldxn;
   float *o_vof, *o_vssf, *o_vtcf;
   long long bins_total;   // entries of the bins region
 };
@@ -1639,8 +1652,10 @@ StaticLayout static_layout(unsigned char* base, int nV, int nT)
   L.acc = (long long*)take(8 * B * kAccLanes);
   L.flags = (int*)take(4 * B);
   L.foldcnt = (int*)take(4 * B * S);
-  L.foldv = (int2*)take(8 * B * GG);
-  L.foldtc = (int*)take(4 * B * GG);
+  L.foldp = (unsigned*)take(4 * B * GG);
+  L.foldtc = (short*)take(2 * B * GG);
+  L.foldx = (FoldEscape*)take(sizeof(FoldEscape) * kFoldEscapes);
+  L.foldxn = (int*)take(4);
   L.foldmeta = (int*)take(4 * B * S * 8);
   L.o_vo = (long long*)take(8 * B); L.o_vss = (long long*)take(8 * B); L.o_vtc = (long long*)take(8 * B);
   L.o_ent = (long long*)take(8 * B); L.o_col = (long long*)take(8 * B);
@@ -1683,8 +1698,9 @@ void static_bind(EngineParams& p, const StaticLayout& L, int nb, int slot, int b
   p.xf = L.xf; p.minkey = L.minkey; p.trange = L.trange;
   p.bin_off = L.bin_off; p.bin_cur = L.bin_cur; p.bins = L.bins; p.bin_cap = bin_cap;
   p.acc = L.acc; p.flags = L.flags; p.bbox = L.bbox; p.bedf = L.bedf;
-  p.foldcnt = L.foldcnt; p.foldv = L.foldv; p.foldmeta = L.foldmeta;
+  p.foldcnt = L.foldcnt; p.foldp = L.foldp; p.foldmeta = L.foldmeta;
   p.foldtc = p.explicit_ss ? nullptr : L.foldtc;
+  p.foldx = L.foldx; p.foldxn = L.foldxn;
   p.out_vo = L.o_vo; p.out_vss = L.o_vss; p.out_vtc = L.o_vtc; p.out_vof = L.o_vof; p.out_vssf = L.o_vssf;
   p.out_vtcf = L.o_vtcf; p.out_nbed = L.o_nbed; p.out_flags = L.o_flags; p.out_entries = L.o_ent;
   p.out_columns = L.o_col;
@@ -1870,6 +1886,8 @@ extern "C" int tomoSweepStatic(const float* f32info, const int* i32info, const f
       if (fl & kFlagSafeOverflow) return set_error(TOMO_ERR_CAPACITY, "column strip exceeds shared memory");
       if (fl & kFlagGrid) return set_error(TOMO_ERR_CAPACITY, "slot index outside the grid");
       if (fl & kFlagRedo) return set_error(TOMO_ERR_CAPACITY, "orientation unresolved after the re-runs");
+      if (fl & kFlagFoldRange)
+        return set_error(TOMO_ERR_CAPACITY, "column values past 16 bits overflowed the fold escape table");
     }
     TOMO_CUDA(cudaMemcpyAsync(g_static_hvof, L.o_vof, sizeof(float) * nb, cudaMemcpyDeviceToHost, st));
     TOMO_CUDA(cudaMemcpyAsync(g_static_hvssf, L.o_vssf, sizeof(float) * nb, cudaMemcpyDeviceToHost, st));
@@ -1993,7 +2011,8 @@ struct MultiEngine {
       v.insert(v.end(), {q.xf.ptr, q.minkey.ptr, q.trange.ptr, q.bin_off.ptr, q.bin_cur.ptr, q.bins.ptr, q.bbox.ptr,
                          q.bedf.ptr});
     for (const auto& st : W.set) {
-      v.insert(v.end(), {st.acc.ptr, st.flags.ptr, st.foldcnt.ptr, st.foldv.ptr, st.foldtc.ptr, st.foldmeta.ptr});
+      v.insert(v.end(), {st.acc.ptr, st.flags.ptr, st.foldcnt.ptr, st.foldp.ptr, st.foldtc.ptr, st.foldx.ptr, st.foldxn.ptr,
+                         st.foldmeta.ptr});
     }
     for (const Engine* e : meshes) {
       v.insert(v.end(), {e->vpos.ptr, e->vnrm.ptr, e->tri.ptr, e->rot.ptr, e->ori.ptr, e->o_vo.ptr, e->o_vss.ptr,

@@ -75,6 +75,7 @@ __device__ __forceinline__ int key_nz(unsigned k) { return (int)(k & 0xFFFFu) - 
 // float -> int16 the way SetBit stores z and nz (STomoVoxelSpaceInfo.cpp:179-180).
 __device__ __forceinline__ int to_i16(float f) { return (int)(short)__float2int_rz(f); }
 
+
 struct TriGeo {
   float ax, ay, az, bx, by, bz, cx, cy, cz;  // translated + margined vertices
   float n0, n1, n2;                          // rotated vertex-normal z
@@ -257,6 +258,7 @@ __global__ void k_reset(EngineParams p)
     p.flags[o] = 0;
     p.bbox[o * 4 + 0] = INT_MAX; p.bbox[o * 4 + 1] = INT_MAX;
     p.bbox[o * 4 + 2] = -1; p.bbox[o * 4 + 3] = -1;
+    if (o == 0) *p.foldxn = 0;
   }
   if (threadIdx.x < 4) p.minkey[o * 4 + threadIdx.x] = f2key(1e5f);  // STomoAABB3Df::Init
   for (int s = threadIdx.x; s <= p.S; s += blockDim.x) p.bin_off[(size_t)o * (p.S + 1) + s] = 0;
@@ -1281,14 +1283,24 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 1) k_strip(EngineParams p
   // columns of one or two raw entries -- almost all of them -- on the spot;
   // longer columns are queued and B2 takes them one per thread, so that the
   // few long lists do not hold up the lanes of the short ones.
-  long long a_vo = 0, a_vss = 0, a_tc = 0, a_avss = 0, a_atc = 0, a_ent = 0, a_col = 0;
+  // per-thread sums over at most H*G columns of |value| <= 2 * grid: int32
+  int a_vo = 0, a_vss = 0, a_tc = 0, a_avss = 0, a_atc = 0, a_ent = 0, a_col = 0;
   int bx0 = INT_MAX, by0 = INT_MAX, bx1 = -1, by1 = -1;
   const bool dump = (o == p.dump_slot) && p.dump_cols != nullptr;
-  int2* fv = p.foldv + (size_t)o * p.G * p.G + (size_t)xs0 * p.G;
-  int* ftc = p.foldtc ? p.foldtc + (size_t)o * p.G * p.G + (size_t)xs0 * p.G : nullptr;
+  unsigned* fv = p.foldp + (size_t)o * p.G * p.G + (size_t)xs0 * p.G;
+  short* ftc = p.foldtc ? p.foldtc + (size_t)o * p.G * p.G + (size_t)xs0 * p.G : nullptr;
   auto store = [&](int l, int ls, int gx, int gy, int gslot, const ColOut& c) {
-    fv[l] = make_int2(c.vo, c.vss);
-    if (ftc) ftc[l] = c.tc;   // tc is zero with explicit support
+    const int lim = p.fold_lim;
+    if (max(max((unsigned)(c.vo + lim), (unsigned)(c.vss + lim)), (unsigned)(c.tc + lim)) <= 2u * (unsigned)lim) {
+      fv[l] = ((unsigned)c.vo & 0xFFFFu) | ((unsigned)c.vss << 16);
+      if (ftc) ftc[l] = (short)c.tc;   // tc is zero with explicit support
+    } else {
+      fv[l] = kFoldEscaped;
+      if (ftc) ftc[l] = 0;
+      const int k = atomicAdd(p.foldxn, 1);
+      if (k < kFoldEscapes) p.foldx[k] = FoldEscape{o, xs0 * p.G + l, c.vo, c.vss, c.tc, 0, 0, 0};
+      else atomicOr(&p.flags[o], kFlagFoldRange);
+    }
     a_vo += c.vo; a_vss += c.vss; a_tc += c.tc;
     a_avss += (c.vss < 0) ? -c.vss : c.vss; a_atc += (c.tc < 0) ? -c.tc : c.tc;
     a_ent += c.ndist;
@@ -1379,7 +1391,7 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 1) k_strip(EngineParams p
   }
 
   // ---- phase C: reductions
-  long long vals[8] = {a_vo, a_vss, a_tc, a_avss, a_atc, a_ent, a_col, 0};
+  const long long vals[8] = {a_vo, a_vss, a_tc, a_avss, a_atc, a_ent, a_col, 0};
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
   for (int k = 0; k < 7; k++) {
@@ -1480,15 +1492,17 @@ __global__ void __launch_bounds__(256) k_bed(EngineParams p)
 // and absolute sums written by k_strip bound every partial sum inside a
 // strip, so whole strips are skipped exactly until the first strip where the
 // bound could pass 2^24; from there the fold is replayed value by value in
-// slot order (staged through shared memory, folded by one thread).  One CTA
-// per orientation.
+// slot order: warps 1-3 unpack the next piece of fold records (and any
+// escaped values) to floats in shared memory while one thread of warp 0 folds
+// the current piece.  One CTA per orientation.
 
-constexpr int kFoldChunk = 1024;
+constexpr int kFoldChunk = 512;
 
 __global__ void __launch_bounds__(128) k_fold(EngineParams p)
 {
-  __shared__ int2 stage[kFoldChunk];
-  __shared__ int stage_tc[kFoldChunk];
+  // two staging buffers: warp 0 folds one while warps 1-3 fill the other
+  __shared__ float2 stage[2][kFoldChunk];    // (vo, vss) of each record, as floats
+  __shared__ float stage_tc[2][kFoldChunk];  // tc (implicit support only)
   __shared__ int s_start;
   __shared__ float s_f[3];
   const int o = blockIdx.x;
@@ -1499,6 +1513,7 @@ __global__ void __launch_bounds__(128) k_fold(EngineParams p)
   if (fl & kFlagRedo) return;
   const long long* a = p.acc + (size_t)o * kAccLanes;
   const int* meta = p.foldmeta + (size_t)o * p.S * 8;
+  const int* cnt = p.foldcnt + (size_t)o * p.S;
   const long long lim = 1ll << 24;
   if (threadIdx.x == 0) {
     p.out_vo[id] = a[kAccVo]; p.out_vss[id] = a[kAccVss]; p.out_vtc[id] = a[kAccVtc];
@@ -1521,28 +1536,53 @@ __global__ void __launch_bounds__(128) k_fold(EngineParams p)
     for (int c = 0; c < 3; c++) s_f[c] = (float)pre[c];
   }
   __syncthreads();
-  const int start = s_start;
+  const bool with_tc = p.foldtc != nullptr;   // tc is zero with explicit support: its fold stays put
+  // the records from strip s_start on, in kFoldChunk pieces
+  auto advance = [&](int& s, int& c0) {
+    while (s < p.S && c0 >= cnt[s]) { s++; c0 = 0; }
+  };
+  auto fill = [&](int s, int c0, int buf, int t0, int nt) {
+    const int m = min(kFoldChunk, cnt[s] - c0);
+    const size_t base = (size_t)o * p.G * p.G + (size_t)s * p.H * p.G + c0;
+    for (int k = t0; k < m; k += nt) {
+      const unsigned x = p.foldp[base + k];
+      int vo = (int)(short)(x & 0xFFFFu), vss = (int)x >> 16, tc = with_tc ? p.foldtc[base + k] : 0;
+      if (x == kFoldEscaped) {
+        const int pos = s * p.H * p.G + c0 + k;
+        const int ne = min(*p.foldxn, kFoldEscapes);
+        for (int e = 0; e < ne; e++)
+          if (p.foldx[e].o == o && p.foldx[e].pos == pos) { vo = p.foldx[e].vo; vss = p.foldx[e].vss; tc = p.foldx[e].tc; break; }
+      }
+      stage[buf][k] = make_float2((float)vo, (float)vss);
+      if (with_tc) stage_tc[buf][k] = (float)tc;
+    }
+  };
   float fo = s_f[0], fs = s_f[1], ft = s_f[2];
-  for (int s = start; s < p.S; s++) {
-    const int n = p.foldcnt[(size_t)o * p.S + s];
-    const int2* v = p.foldv + (size_t)o * p.G * p.G + (size_t)s * p.H * p.G;
-    const int* vt = p.foldtc ? p.foldtc + (size_t)o * p.G * p.G + (size_t)s * p.H * p.G : nullptr;
-    for (int c0 = 0; c0 < n; c0 += kFoldChunk) {
-      const int m = min(kFoldChunk, n - c0);
-      __syncthreads();
-      for (int k = threadIdx.x; k < m; k += blockDim.x) {
-        stage[k] = v[c0 + k];
-        stage_tc[k] = vt ? vt[c0 + k] : 0;
-      }
-      __syncthreads();
+  int s = s_start, c0 = 0, buf = 0;
+  advance(s, c0);
+  if (s < p.S) {
+    fill(s, c0, 0, threadIdx.x, blockDim.x);
+    __syncthreads();
+    while (true) {
+      int s1 = s, c1 = c0 + kFoldChunk;
+      advance(s1, c1);
       if (threadIdx.x == 0) {
-        for (int k = 0; k < m; k++) {
-          const int2 x = stage[k];
-          fo = __fadd_rn(fo, (float)x.x);
-          fs = __fadd_rn(fs, (float)x.y);
-          ft = __fadd_rn(ft, (float)stage_tc[k]);
+        const int m = min(kFoldChunk, cnt[s] - c0);
+        const float2* st = stage[buf];
+        if (with_tc) {
+          for (int k = 0; k < m; k++) {
+            fo = __fadd_rn(fo, st[k].x); fs = __fadd_rn(fs, st[k].y); ft = __fadd_rn(ft, stage_tc[buf][k]);
+          }
+        } else {
+#pragma unroll 8
+          for (int k = 0; k < m; k++) { fo = __fadd_rn(fo, st[k].x); fs = __fadd_rn(fs, st[k].y); }
         }
+      } else if (threadIdx.x >= 32 && s1 < p.S) {
+        fill(s1, c1, buf ^ 1, threadIdx.x - 32, blockDim.x - 32);
       }
+      __syncthreads();
+      if (s1 >= p.S) break;
+      s = s1; c0 = c1; buf ^= 1;
     }
   }
   if (threadIdx.x == 0) {

@@ -25,6 +25,7 @@ _i64p = ct.POINTER(ct.c_int64)
 TOMO_OPT_BATCH, TOMO_OPT_STRIP_H, TOMO_OPT_FORCE_SAFE, TOMO_OPT_NORMAL_SMEM, TOMO_OPT_EXPORT = 1, 2, 3, 4, 5
 TOMO_OPT_ADAPTIVE = 6
 TOMO_OPT_PROPOSAL = 7
+TOMO_OPT_FOLD_LIMIT = 8
 
 # (name, restype, argtypes) for every export of include/tomo_b200.h
 EXPORTS = [
