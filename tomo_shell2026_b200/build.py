@@ -22,7 +22,7 @@ INCLUDE = PKG.parent / "include"
 NVCC = os.environ.get("NVCC", str(Path(os.environ.get("CUDA_HOME", "/usr/local/cuda")) / "bin" / "nvcc"))
 
 SOURCES = ["tomo_kernels.cu", "tomo_engine.cu", "tomo_mlp.cu"]
-HEADERS = ["tomo_common.cuh", "tomo_mlp.cuh"]
+HEADERS = ["tomo_common.cuh", "tomo_mlp.cuh", "tomo_span.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

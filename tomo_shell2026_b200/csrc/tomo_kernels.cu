@@ -22,6 +22,7 @@
 //
 // No kernel waits on another CTA; every shared and global index is checked.
 #include "tomo_common.cuh"
+#include "tomo_span.cuh"
 
 #include <climits>
 
@@ -165,7 +166,7 @@ __device__ __forceinline__ float centroid(float a, float b, float c)
 // u >= 0 and u + v <= 1 + 2^-23, inside every bound of the test).  Only
 // pixels in the thin band between run the exact test.  The pixel nearest
 // the centroid is tried first: for all but the smallest triangles it is
-// inside, and the box scan is skipped.
+// inside, and the box scan is skipped; the scan visits only the row spans.
 __device__ bool any_hit(const EngineParams& p, const TriGeo& g, const Bary& b)
 {
   if (!b.ok) return false;
@@ -200,9 +201,18 @@ __device__ bool any_hit(const EngineParams& p, const TriGeo& g, const Bary& b)
     const int y = min(max(__float2int_rd(my - p.half), g.y0), g.y1);
     if (hit(x, y)) return true;
   }
-  for (int x = g.x0; x <= g.x1; x++)
-    for (int y = g.y0; y <= g.y1; y++)
+  // Scan only the rows of each column whose centres can pass the pre-reject
+  // (tomo_span.cuh); a box whose spans are all empty holds no hit.  With a
+  // (nearly) zero slope the spans are not formed and the whole box is scanned.
+  const int ylen = g.y1 - g.y0 + 1;
+  const SpanTri T = span_setup(g.ax, g.ay, b.e0x, b.e0y, b.e1x, b.e1y, b.d00, b.d01, b.d11, dpos, rlo, ruhi, g.x0,
+                               g.x1, g.y0, ylen, p.half);
+  for (int x = g.x0; x <= g.x1; x++) {
+    int lo = g.y0, hi = g.y1;
+    if (T.ok) span_rows(T, pix_center(x, p.half), g.y0, ylen, lo, hi);
+    for (int y = lo; y <= hi; y++)
       if (hit(x, y)) return true;
+  }
   return false;
 }
 
