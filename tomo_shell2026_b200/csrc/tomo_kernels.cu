@@ -195,10 +195,11 @@ __device__ bool any_hit(const EngineParams& p, const TriGeo& g, const Bary& b)
     return bary_test(g.ax, g.ay, b, px, py, p.vmax, u, v, w);
   };
   {
-    // a guess only (any pixel of the box would do), so its rounding does not matter
+    // the pixel whose centre (x + 0.001 + half) is nearest the centroid; a
+    // guess only (any pixel of the box would do), so its rounding does not matter
     const float mx = (g.ax + g.bx + g.cx) * (1.0f / 3.0f), my = (g.ay + g.by + g.cy) * (1.0f / 3.0f);
-    const int x = min(max(__float2int_rd(mx - p.half), g.x0), g.x1);
-    const int y = min(max(__float2int_rd(my - p.half), g.y0), g.y1);
+    const int x = min(max(__float2int_rd(mx - p.half + 0.499f), g.x0), g.x1);
+    const int y = min(max(__float2int_rd(my - p.half + 0.499f), g.y0), g.y1);
     if (hit(x, y)) return true;
   }
   // Scan only the rows of each column whose centres can pass the pre-reject
