@@ -284,35 +284,55 @@ __global__ void k_reset(EngineParams p)
 // atomics.  Only the normal's z component is kept: it is the only one the
 // INT3 path reads (SetBit uses nrm[2]).
 
+// One thread per vertex and kRotGroup orientations: the vertex is loaded
+// once and rotated by each orientation of the group (independent chains for
+// the scheduler), the group's matrices sit in shared memory, and the AABB
+// minima are reduced per warp, then per block, before one atomic each.
+constexpr int kRotGroup = 8;
+
 __global__ void __launch_bounds__(256) k_rotate(EngineParams p)
 {
-  const int o = blockIdx.y;
-  const float* R = p.rot + (size_t)p.ori[o] * 9;
-  const float r00 = R[0], r01 = R[1], r02 = R[2], r10 = R[3], r11 = R[4], r12 = R[5];
-  const float r20 = R[6], r21 = R[7], r22 = R[8];
-  float mx = 1e5f, my = 1e5f, mz = 1e5f;
-  float4* out = p.xf + (size_t)o * p.nV;
-  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < p.nV; v += gridDim.x * blockDim.x) {
-    const float4 a = p.vpos[v];
-    const float4 n = p.vnrm[v];
-    const float t0 = __fsub_rn(a.x, p.cx), t1 = __fsub_rn(a.y, p.cy), t2 = __fsub_rn(a.z, p.cz);
-    const float x = row_dot(r00, r01, r02, t0, t1, t2);
-    const float y = row_dot(r10, r11, r12, t0, t1, t2);
-    const float z = row_dot(r20, r21, r22, t0, t1, t2);
-    const float nz = row_dot(r20, r21, r22, n.x, n.y, n.z);
-    out[v] = make_float4(x, y, z, nz);
-    mx = fmin_ref(mx, x); my = fmin_ref(my, y); mz = fmin_ref(mz, z);
+  __shared__ float rm[kRotGroup][9];
+  __shared__ unsigned kmin[kRotGroup][3];
+  const int o0 = blockIdx.y * kRotGroup;
+  const int ng = min(kRotGroup, p.Bo - o0);
+  if (threadIdx.x < kRotGroup * 9) {
+    const int k = threadIdx.x / 9, e = threadIdx.x % 9;
+    rm[k][e] = k < ng ? p.rot[(size_t)p.ori[o0 + k] * 9 + e] : 0.0f;
   }
-  for (int off = 16; off > 0; off >>= 1) {
-    mx = fmin_ref(mx, __shfl_xor_sync(0xFFFFFFFFu, mx, off));
-    my = fmin_ref(my, __shfl_xor_sync(0xFFFFFFFFu, my, off));
-    mz = fmin_ref(mz, __shfl_xor_sync(0xFFFFFFFFu, mz, off));
+  if (threadIdx.x < kRotGroup * 3) kmin[threadIdx.x / 3][threadIdx.x % 3] = 0xFFFFFFFFu;
+  __syncthreads();
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  float4 a = make_float4(0.f, 0.f, 0.f, 0.f), n = a;
+  if (v < p.nV) { a = p.vpos[v]; n = p.vnrm[v]; }
+  const float t0 = __fsub_rn(a.x, p.cx), t1 = __fsub_rn(a.y, p.cy), t2 = __fsub_rn(a.z, p.cz);
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int k = 0; k < kRotGroup; k++) {
+    if (k >= ng) break;   // block-uniform
+    const float* R = rm[k];
+    float x = row_dot(R[0], R[1], R[2], t0, t1, t2);
+    float y = row_dot(R[3], R[4], R[5], t0, t1, t2);
+    float z = row_dot(R[6], R[7], R[8], t0, t1, t2);
+    if (v < p.nV) {
+      const float nz = row_dot(R[6], R[7], R[8], n.x, n.y, n.z);
+      p.xf[(size_t)(o0 + k) * p.nV + v] = make_float4(x, y, z, nz);
+    } else {
+      x = y = z = 1e5f;   // STomoAABB3Df::Init
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+      x = fmin_ref(x, __shfl_xor_sync(0xFFFFFFFFu, x, off));
+      y = fmin_ref(y, __shfl_xor_sync(0xFFFFFFFFu, y, off));
+      z = fmin_ref(z, __shfl_xor_sync(0xFFFFFFFFu, z, off));
+    }
+    if (lane == 0) {
+      atomicMin(&kmin[k][0], f2key(x));
+      atomicMin(&kmin[k][1], f2key(y));
+      atomicMin(&kmin[k][2], f2key(z));
+    }
   }
-  if ((threadIdx.x & 31) == 0) {
-    atomicMin(&p.minkey[o * 4 + 0], f2key(mx));
-    atomicMin(&p.minkey[o * 4 + 1], f2key(my));
-    atomicMin(&p.minkey[o * 4 + 2], f2key(mz));
-  }
+  __syncthreads();
+  if (threadIdx.x < ng * 3) atomicMin(&p.minkey[(o0 + threadIdx.x / 3) * 4 + threadIdx.x % 3], kmin[threadIdx.x / 3][threadIdx.x % 3]);
 }
 
 // ---------------------------------------------------------------- K2 binning
@@ -1748,17 +1768,13 @@ static dim3 tri_grid(const EngineParams& p)
   return dim3(b > 0 ? b : 1, p.Bo);
 }
 
-static dim3 vtx_grid(const EngineParams& p)
-{
-  const int b = (p.nV + 255) / 256 < 64 ? (p.nV + 255) / 256 : 64;
-  return dim3(b > 0 ? b : 1, p.Bo);
-}
-
 // Count pass of one batch (reset, rotate, bin count, bin scan).
 cudaError_t launch_bin_count(const EngineParams& p, cudaStream_t main, LaunchLog* L)
 {
   TOMO_LAUNCH(kKReset, main, (k_reset<<<p.Bo, 256, 0, main>>>(p)));
-  TOMO_LAUNCH(kKRotate, main, (k_rotate<<<vtx_grid(p), 256, 0, main>>>(p)));
+  TOMO_LAUNCH(kKRotate, main,
+              (k_rotate<<<dim3((p.nV + 255) / 256 > 0 ? (p.nV + 255) / 256 : 1, (p.Bo + kRotGroup - 1) / kRotGroup), 256,
+                           0, main>>>(p)));
   TOMO_LAUNCH(kKCount, main, (k_bin_count<<<tri_grid(p), 256, sizeof(int) * p.S, main>>>(p)));
   TOMO_LAUNCH(kKScan, main, (k_bin_scan<<<p.Bo, 1024, 0, main>>>(p)));
   return cudaGetLastError();
