@@ -185,6 +185,9 @@ def test_fold_escape_table(oracle, explicit_ss):
     assert 1 <= lim < int(mag[0]) and np.count_nonzero(mag > lim) <= 600
     want = oracle.sweep(m, ypr, opts, grid=G)
     assert int(want["Vo64"][0]) > (1 << 24)
+    for bad in (0, -5, 32768):
+        with pytest.raises(native.TomoError):
+            native.set_option(native.TOMO_OPT_FOLD_LIMIT, bad)
     try:
         native.set_option(native.TOMO_OPT_FOLD_LIMIT, lim)
         res = native.sweep(m, ypr, opts)
