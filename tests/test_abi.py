@@ -38,6 +38,17 @@ def test_library_exports_every_declared_symbol():
     assert set(declared_functions()) <= bound, "native.EXPORTS lacks a declared function"
 
 
+def test_option_keys_match_the_header():
+    """The option keys native.py passes to tomoSetOption are the header's."""
+    text = HEADER.read_text()
+    defines = {m.group(1): int(m.group(2)) for m in re.finditer(r"#define\s+(TOMO_\w+)\s+(-?\d+)", text)}
+    opts = {k: v for k, v in defines.items() if k.startswith("TOMO_OPT_")}
+    assert opts, "no TOMO_OPT_ keys in the header"
+    for name, value in opts.items():
+        assert getattr(native, name) == value, f"native.{name} != {value}"
+    assert len(set(opts.values())) == len(opts), "option keys collide"
+
+
 def bits(a):
     a = np.asarray(a)
     return a.view(np.int32) if a.dtype == np.float32 else a
