@@ -502,7 +502,7 @@ __global__ void __launch_bounds__(256) k_bin_fill(EngineParams p)
 // (triangle, pixel, twin) priority of every entry.
 
 constexpr int kChunk = 256;    // triangles staged per pass (== blockDim.x)
-constexpr int kRegKeys = 10;   // columns with up to this many raw pixels sort in registers
+constexpr int kRegKeys = 11;   // columns with up to this many raw pixels sort in registers
 constexpr int kMaxEnt = 32767; // entry indices are stored as int16
 constexpr int kWarpKeys = 64;  // raw entries a warp sorts in registers (two per lane)
 constexpr int kWalkQueue = 64; // pre-reject survivors queued per warp before the exact test
